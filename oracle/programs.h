@@ -1,0 +1,82 @@
+/*
+ * Datalog programs written once against parallel-RA's public C++ API
+ * (relation, RAM, parallel_join, parallel_copy, parallel_copy_filter), so the
+ * same source builds on the reference library (oracle/_ref/ref_driver) and on
+ * the B200 library's source-compatible headers (parallel-ra_b200/cxx).
+ *
+ * TEST INFRASTRUCTURE: these builders feed the parity drivers.
+ *
+ *  - tc: exactly the rule set of tests/transitive_closure.cpp:56-77 (T stored
+ *        as (dst,src); copy G {1,0}; join T DELTA x G FULL {3,1}).
+ *  - sg: same generation over a parent->child edge relation:
+ *        SGB(x,y)  :- edge(p,x), edge(p,y).               (join E FULL x E FULL)
+ *        SG(x,y)   :- SGB(x,y), x != y.                   (copy_filter)
+ *        TMP(b,x)  :- SG(a,b), edge(a,x).                 (join SG DELTA x E FULL)
+ *        SG(x,y)   :- TMP(b,x), edge(b,y).                (join TMP DELTA x E FULL)
+ *        The reference's join carries no filter (src/RA/parallel_join.h:55), so
+ *        the base rule is a join into SGB followed by a filtering copy.
+ */
+#pragma once
+#include <string>
+#include <vector>
+#include <utility>
+
+struct ra_program_def {
+    std::vector<relation*> relations;
+    std::vector<RAM*> sccs;                          /* in add_scc order */
+    std::vector<std::pair<RAM*, RAM*>> deps;        /* (src, dst): src runs first */
+};
+
+/* tests/transitive_closure.cpp:56-77 */
+inline void build_tc(ra_program_def& p, const std::string& edge_file, const std::string& empty_file)
+{
+    relation* T = new relation(1, true, 2, 257, "T", empty_file, FULL);
+    relation* G = new relation(1, true, 2, 256, "G", edge_file, FULL);
+
+    RAM* scc_join = new RAM(true, 1);
+    scc_join->add_relation(G, false);
+    scc_join->add_relation(T, true);
+    scc_join->add_rule(new parallel_join(T, T, DELTA, G, FULL, {3, 1}));
+
+    RAM* scc_copy = new RAM(false, 2);
+    scc_copy->add_relation(G, false);
+    scc_copy->add_relation(T, true);
+    scc_copy->add_rule(new parallel_copy(T, G, FULL, {1, 0}));
+
+    p.relations = {T, G};
+    p.sccs = {scc_join, scc_copy};
+    p.deps = {{scc_copy, scc_join}};
+}
+
+inline bool sg_distinct(const u64* const data) { return data[0] != data[1]; }
+
+inline void build_sg(ra_program_def& p, const std::string& edge_file, const std::string& empty_file)
+{
+    relation* E   = new relation(1, true, 2, 300, "edge", edge_file, FULL);
+    relation* SGB = new relation(1, true, 2, 301, "SGB", empty_file, FULL);
+    relation* SG  = new relation(1, true, 2, 302, "SG", empty_file, FULL);
+    relation* TMP = new relation(1, true, 2, 303, "TMP", empty_file, FULL);
+
+    /* (p, x, idE, y, idE') -> (x, y) */
+    RAM* scc_base = new RAM(false, 10);
+    scc_base->add_relation(E, false);
+    scc_base->add_relation(SGB, true);
+    scc_base->add_rule(new parallel_join(SGB, E, FULL, E, FULL, {1, 3}));
+
+    RAM* scc_filter = new RAM(false, 11);
+    scc_filter->add_relation(SGB, false);
+    scc_filter->add_relation(SG, true);
+    scc_filter->add_rule(new parallel_copy_filter(SG, SGB, FULL, {0, 1}, sg_distinct));
+
+    /* (a, b, idS, x, idE) -> (b, x);  (b, x, idT, y, idE) -> (x, y) */
+    RAM* scc_rec = new RAM(true, 12);
+    scc_rec->add_relation(E, false);
+    scc_rec->add_relation(SG, true);
+    scc_rec->add_relation(TMP, false);
+    scc_rec->add_rule(new parallel_join(TMP, SG, DELTA, E, FULL, {1, 3}));
+    scc_rec->add_rule(new parallel_join(SG, TMP, DELTA, E, FULL, {1, 3}));
+
+    p.relations = {E, SGB, SG, TMP};
+    p.sccs = {scc_base, scc_filter, scc_rec};
+    p.deps = {{scc_base, scc_filter}, {scc_filter, scc_rec}};
+}
