@@ -1,0 +1,146 @@
+/*
+ * parallel-RA on B200: C ABI of the device engine.
+ *
+ * One ra_program holds the relations, SCCs (strongly connected components,
+ * the reference's RAM tasks) and rules of one Datalog program, all resident on
+ * one GPU.  The C++ classes relation / RAM / parallel_join / parallel_copy /
+ * parallel_copy_filter / LIE in parallel-ra_b200/cxx are thin builders over
+ * these calls, so programs written against parallel-RA's C++ API
+ * (e.g. tests/transitive_closure.cpp) compile unchanged.
+ *
+ * Conventions: every call returns an ra_status (0 = RA_OK).  Relations and
+ * SCCs are small integer handles local to their program.  Tuples cross the
+ * ABI as rows of arity+1 uint64 (data columns, then the intern id column),
+ * the layout of the reference's binary relation files
+ * (utility/tsv_to_bin.cpp:38-64, src/IO/parallel_io.cpp:115-213).
+ * Calls on one program must come from one host thread at a time.
+ */
+#ifndef RA_ENGINE_H
+#define RA_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ra_status {
+    RA_OK = 0,
+    RA_E_BADARG = 1,      /* invalid handle, arity, projection, version ... */
+    RA_E_IO = 2,          /* relation file or its .size metadata unreadable */
+    RA_E_OOM = 3,         /* device allocation failed */
+    RA_E_CUDA = 4,        /* a CUDA runtime call failed (message via ra_last_error) */
+    RA_E_UNSUPPORTED = 5, /* program shape outside what the engine implements */
+    RA_E_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+    RA_E_STATE = 7        /* call made in the wrong phase (e.g. dump before execute) */
+} ra_status;
+
+/* relation versions, src/relation/balanced_hash_relation.h:13 */
+#define RA_DELTA 0
+#define RA_FULL 1
+
+/* copy rule kinds: parallel_copy (src/RA/parallel_copy.h:28),
+ * parallel_acopy (src/RA/parallel_acopy.h:45),
+ * parallel_copy_filter (src/RA/parallel_copy_filter.h:29) */
+#define RA_COPY 0
+#define RA_ACOPY 1
+#define RA_COPY_FILTER 2
+
+/* Device-evaluable copy_filter predicates over input columns 0 and 1 (the
+ * only columns the reference passes to the filter lambda,
+ * src/relation/shmap_relation_exp.cpp:233-236). */
+#define RA_PRED_TRUE 0
+#define RA_PRED_FALSE 1
+#define RA_PRED_EQ 2
+#define RA_PRED_NE 3
+#define RA_PRED_LT 4
+#define RA_PRED_GT 5
+#define RA_PRED_LE 6
+#define RA_PRED_GE 7
+
+typedef struct ra_program ra_program;
+
+/* Per-run statistics of the last ra_program_execute. */
+typedef struct ra_stats {
+    uint64_t iterations;        /* fixed-point iterations over all SCCs */
+    uint64_t join_candidates;   /* sum over iterations of join/copy outputs */
+    uint64_t new_tuples;        /* sum over iterations of tuples added to delta */
+    uint64_t kernel_launches;   /* engine kernels launched by the run */
+    double fixpoint_ms;         /* device time of the SCC loops (CUDA events) */
+    double dedup_ms;            /* device time of the fused join+dedup kernels */
+    uint64_t dedup_launches;    /* launches of those kernels */
+    uint64_t dedup_bytes;       /* algorithmic bytes moved by those kernels */
+    uint32_t value_bits;        /* bits per packed column chosen for the run */
+    uint32_t reserved;
+} ra_stats;
+
+/* Create a program on CUDA device `device`.  Replaces the per-rank set-up of
+ * mpi_comm::create + LIE::LIE (src/comm/comm.cpp:22-30, src/lie/lie.h:67-81). */
+int ra_program_create(int device, ra_program** out);
+int ra_program_destroy(ra_program* p);
+/* Bind the program to an existing CUDA stream (cudaStream_t); 0 = engine's own. */
+int ra_program_set_stream(ra_program* p, void* stream);
+/* Iterations per fixed-point check, LIE::set_batch_size (src/lie/lie.h:111). */
+int ra_program_set_batch_size(ra_program* p, uint32_t batch_size);
+
+/* relation(jcc, is_canonical, arity, tag, name, file, version),
+ * src/relation/balanced_hash_relation.h:97.  arity <= 8. */
+int ra_relation_create(ra_program* p, uint32_t jcc, uint32_t arity, uint32_t tag,
+                       const char* name, int version, int* rel_out);
+/* Initial tuples from host rows (arity+1 u64 each).  Replaces
+ * relation::load_data_from_file + populate_full (balanced_hash_relation.cpp:609-793)
+ * and the load-time all_to_all (src/IO/parallel_io.cpp:239-297). */
+int ra_relation_load_rows(ra_program* p, int rel, const uint64_t* host_rows, uint64_t nrows);
+/* Same, from rows already in device memory (copied; the caller keeps ownership). */
+int ra_relation_load_rows_device(ra_program* p, int rel, const uint64_t* dev_rows, uint64_t nrows);
+/* Same, from a file in the reference's binary format plus "<path>.size"
+ * (parallel_io::parallel_read_input_relation_from_file_to_local_buffer,
+ * src/IO/parallel_io.cpp:115-213). */
+int ra_relation_load_file(ra_program* p, int rel, const char* path);
+
+/* RAM(bool fixpoint, int id), src/RAM/RA_tasks.h:52 */
+int ra_scc_create(ra_program* p, int fixpoint, int scc_id, int* scc_out);
+/* RAM::add_relation(relation*&, bool init_status), src/RAM/RA_tasks.h:75 */
+int ra_scc_add_relation(ra_program* p, int scc, int rel, int init_status);
+/* RAM::add_rule(new parallel_join(out, in0, ver0, in1, ver1, proj)),
+ * src/RA/parallel_join.h:55 */
+int ra_scc_add_join(ra_program* p, int scc, int out, int in0, int ver0, int in1, int ver1,
+                    const int* proj, int nproj);
+/* RAM::add_rule(new parallel_copy / parallel_acopy / parallel_copy_filter(...)),
+ * src/RA/parallel_copy.h:28, parallel_acopy.h:45, parallel_copy_filter.h:29.
+ * pred is an RA_PRED_* code (ignored unless kind == RA_COPY_FILTER). */
+int ra_scc_add_copy(ra_program* p, int scc, int kind, int out, int in, int ver,
+                    const int* proj, int nproj, int pred);
+/* LIE::add_scc_dependance(src, dst), src/lie/lie.h:131 */
+int ra_scc_depend(ra_program* p, int src_scc, int dst_scc);
+
+/* LIE::execute (src/lie/lie.cpp:197-448): run every SCC in dependency order to
+ * its fixed point on the device. */
+int ra_program_execute(ra_program* p);
+/* Return every relation to its loaded state so the program can run again. */
+int ra_program_reset(ra_program* p);
+
+/* Per-SCC history in execution order, flattened as
+ * [scc_id, n, (sum_delta, sum_full) x n] per SCC -- the values that
+ * RAM::check_for_fixed_point pushes (src/RAM/RA_tasks.cpp:1072-1085). */
+int ra_program_history(ra_program* p, uint64_t* out, uint64_t cap, uint64_t* len);
+int ra_program_stats(ra_program* p, ra_stats* out);
+
+/* relation::get_full_element_count / get_delta_element_count
+ * (src/relation/balanced_hash_relation.h:183,206) */
+int ra_relation_counts(ra_program* p, int rel, uint64_t* full, uint64_t* delta);
+/* Full relation rows (arity+1 u64 each) in lexicographic order, the order in
+ * which the reference's trie enumerates them (shmap_relation_exp.cpp:77-112).
+ * Writes min(cap_rows, count) rows to host memory. */
+int ra_relation_dump_full(ra_program* p, int rel, uint64_t* host_rows, uint64_t cap_rows,
+                          uint64_t* rows_out);
+
+const char* ra_status_string(int status);
+/* Message of the last failing call on this program ("" if none). */
+const char* ra_last_error(ra_program* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RA_ENGINE_H */

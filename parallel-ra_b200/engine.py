@@ -1,0 +1,203 @@
+"""ctypes binding of the B200 engine's C ABI (include/ra_engine.h).
+
+``Program`` exposes the builder methods used by ``programs.py`` (relation /
+load_rows / scc / add_relation / join / copy / depend) plus execute, history,
+counts and dumps.  Every call goes to ``libra_b200.so``; there is no host
+fallback: without the library or a GPU the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libra_b200.so")
+
+DELTA, FULL = 0, 1
+COPY, ACOPY, COPY_FILTER = 0, 1, 2
+
+# every entry point declared in include/ra_engine.h
+EXPORTS = (
+    "ra_program_create", "ra_program_destroy", "ra_program_set_stream", "ra_program_set_batch_size",
+    "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
+    "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
+    "ra_program_execute", "ra_program_reset", "ra_program_history", "ra_program_stats",
+    "ra_relation_counts", "ra_relation_dump_full", "ra_status_string", "ra_last_error",
+)
+
+
+class RAError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint64), ("join_candidates", C.c_uint64), ("new_tuples", C.c_uint64),
+        ("kernel_launches", C.c_uint64), ("fixpoint_ms", C.c_double), ("dedup_ms", C.c_double),
+        ("dedup_launches", C.c_uint64), ("dedup_bytes", C.c_uint64), ("value_bits", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libra_b200.so (built by build.py); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run parallel-ra_b200/build.py (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        u64p = C.POINTER(C.c_uint64)
+        i32p = C.POINTER(C.c_int)
+        L.ra_program_create.argtypes = [C.c_int, C.POINTER(P)]
+        L.ra_program_destroy.argtypes = [P]
+        L.ra_program_set_stream.argtypes = [P, P]
+        L.ra_program_set_batch_size.argtypes = [P, C.c_uint32]
+        L.ra_relation_create.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int, i32p]
+        L.ra_relation_load_rows.argtypes = [P, C.c_int, u64p, C.c_uint64]
+        L.ra_relation_load_rows_device.argtypes = [P, C.c_int, C.c_void_p, C.c_uint64]
+        L.ra_relation_load_file.argtypes = [P, C.c_int, C.c_char_p]
+        L.ra_scc_create.argtypes = [P, C.c_int, C.c_int, i32p]
+        L.ra_scc_add_relation.argtypes = [P, C.c_int, C.c_int, C.c_int]
+        L.ra_scc_add_join.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, i32p, C.c_int]
+        L.ra_scc_add_copy.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, i32p, C.c_int, C.c_int]
+        L.ra_scc_depend.argtypes = [P, C.c_int, C.c_int]
+        L.ra_program_execute.argtypes = [P]
+        L.ra_program_reset.argtypes = [P]
+        L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
+        L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
+        L.ra_relation_counts.argtypes = [P, C.c_int, u64p, u64p]
+        L.ra_relation_dump_full.argtypes = [P, C.c_int, u64p, C.c_uint64, u64p]
+        L.ra_status_string.argtypes = [C.c_int]
+        L.ra_status_string.restype = C.c_char_p
+        L.ra_last_error.argtypes = [P]
+        L.ra_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _u64(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint64))
+
+
+class Program:
+    """One Datalog program on one GPU (an ``ra_program``)."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = C.c_void_p()
+        st = self._L.ra_program_create(device, C.byref(h))
+        if st != 0:
+            raise RAError(st, f"ra_program_create(device={device}): {self._L.ra_status_string(st).decode()}")
+        self._p = h
+        self._arity = {}
+
+    def _ck(self, st, what):
+        if st != 0:
+            raise RAError(st, f"{what}: {self._L.ra_status_string(st).decode()}: "
+                              f"{self._L.ra_last_error(self._p).decode()}")
+
+    def close(self):
+        if getattr(self, "_p", None):
+            self._L.ra_program_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._p
+
+    def set_stream(self, stream_ptr: int):
+        self._ck(self._L.ra_program_set_stream(self._p, C.c_void_p(stream_ptr)), "set_stream")
+
+    def set_batch_size(self, n: int):
+        self._ck(self._L.ra_program_set_batch_size(self._p, n), "set_batch_size")
+
+    def relation(self, jcc, arity, tag, name, version=FULL):
+        out = C.c_int()
+        self._ck(self._L.ra_relation_create(self._p, jcc, arity, tag, name.encode(), version, C.byref(out)),
+                 "relation")
+        self._arity[out.value] = arity
+        return out.value
+
+    def load_rows(self, rel, rows: np.ndarray):
+        rows = np.ascontiguousarray(rows, dtype=np.uint64)
+        self._ck(self._L.ra_relation_load_rows(self._p, rel, _u64(rows), rows.shape[0]), "load_rows")
+
+    def load_rows_device(self, rel, dev_ptr: int, nrows: int):
+        self._ck(self._L.ra_relation_load_rows_device(self._p, rel, C.c_void_p(dev_ptr), nrows), "load_rows_device")
+
+    def load_file(self, rel, path: str):
+        self._ck(self._L.ra_relation_load_file(self._p, rel, path.encode()), "load_file")
+
+    def scc(self, fixpoint, scc_id):
+        out = C.c_int()
+        self._ck(self._L.ra_scc_create(self._p, int(bool(fixpoint)), scc_id, C.byref(out)), "scc")
+        return out.value
+
+    def add_relation(self, scc, rel, init_status):
+        self._ck(self._L.ra_scc_add_relation(self._p, scc, rel, int(bool(init_status))), "add_relation")
+
+    def join(self, scc, out, in0, ver0, in1, ver1, proj):
+        arr = (C.c_int * len(proj))(*proj)
+        self._ck(self._L.ra_scc_add_join(self._p, scc, out, in0, ver0, in1, ver1, arr, len(proj)), "join")
+
+    def copy(self, scc, out, src, ver, proj, kind=COPY, pred=0):
+        arr = (C.c_int * len(proj))(*proj)
+        self._ck(self._L.ra_scc_add_copy(self._p, scc, kind, out, src, ver, arr, len(proj), pred), "copy")
+
+    def depend(self, src_scc, dst_scc):
+        self._ck(self._L.ra_scc_depend(self._p, src_scc, dst_scc), "depend")
+
+    def execute(self, batch_size: int | None = None):
+        if batch_size is not None:
+            self.set_batch_size(batch_size)
+        self._ck(self._L.ra_program_execute(self._p), "execute")
+
+    def reset(self):
+        self._ck(self._L.ra_program_reset(self._p), "reset")
+
+    def history(self):
+        """[(scc_id, [(sum_delta, sum_full), ...]), ...] in execution order."""
+        n = C.c_uint64()
+        self._ck(self._L.ra_program_history(self._p, None, 0, C.byref(n)), "history")
+        buf = np.zeros(max(n.value, 1), dtype=np.uint64)
+        self._ck(self._L.ra_program_history(self._p, _u64(buf), n.value, C.byref(n)), "history")
+        out, i = [], 0
+        while i < n.value:
+            sid, k = int(buf[i]), int(buf[i + 1])
+            pairs = [(int(buf[i + 2 + 2 * j]), int(buf[i + 3 + 2 * j])) for j in range(k)]
+            out.append((sid, pairs))
+            i += 2 + 2 * k
+        return out
+
+    def stats(self) -> Stats:
+        s = Stats()
+        self._ck(self._L.ra_program_stats(self._p, C.byref(s)), "stats")
+        return s
+
+    def counts(self, rel):
+        f, d = C.c_uint64(), C.c_uint64()
+        self._ck(self._L.ra_relation_counts(self._p, rel, C.byref(f), C.byref(d)), "counts")
+        return f.value, d.value
+
+    def full_count(self, rel):
+        return self.counts(rel)[0]
+
+    def dump_full(self, rel):
+        """Full relation rows (data columns + id) in lexicographic order."""
+        n = self.full_count(rel)
+        w = self._arity[rel] + 1
+        buf = np.zeros((max(n, 1), w), dtype=np.uint64)
+        got = C.c_uint64()
+        self._ck(self._L.ra_relation_dump_full(self._p, rel, _u64(buf), n, C.byref(got)), "dump_full")
+        return buf[:got.value]

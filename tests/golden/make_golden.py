@@ -1,0 +1,114 @@
+"""Generate the golden vectors in tests/golden/ from the reference itself.
+
+Runs oracle/_ref/ref_driver (the unchanged parallel-RA sources built by
+oracle/Makefile against a single-rank MPI stand-in) on
+  * the reference's own fixtures data/g5955/edge_2_1_2 and
+    data/g13236/edge_2_1_2 (copied here as fixtures), and
+  * seeded synthetic graphs (TC on Erdos-Renyi graphs, SG on random trees),
+and records, per case, the per-SCC history of (sum |delta|, sum |full|)
+pairs, every relation's full count, and a SHA-256 of each relation's sorted
+rows (data columns + intern id).  Small relations are also stored verbatim.
+
+Needs the reference tree (default /root/reference); run from the repo root:
+    python tests/golden/make_golden.py [--ref /root/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+import parallel_ra_b200 as P  # noqa: E402
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+
+# (name, program, source) -- source is a reference fixture path or a generator spec
+CASES = [
+    ("g5955_tc", "tc", ("fixture", "g5955")),
+    ("g13236_tc", "tc", ("fixture", "g13236")),
+    ("er200_tc", "tc", ("er", 200, 300, 7)),
+    ("er2000_tc", "tc", ("er", 2000, 3000, 1)),
+    ("er20000_tc", "tc", ("er", 20000, 19000, 3)),
+    ("tree256_sg", "sg", ("tree", 256, 11)),
+    ("tree1024_sg", "sg", ("tree", 1024, 5)),
+]
+VERBATIM_MAX_ROWS = 4096
+
+
+def rows_digest(rows: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(rows, dtype="<u8").tobytes()).hexdigest()
+
+
+def input_rows(src, ref_root):
+    kind = src[0]
+    if kind == "fixture":
+        return P.datagen.read_relation(os.path.join(ref_root, "data", src[1], "edge_2_1_2"))
+    if kind == "er":
+        return P.datagen.with_row_ids(P.datagen.erdos_renyi(src[1], src[2], src[3]))
+    if kind == "tree":
+        return P.datagen.with_row_ids(P.datagen.random_tree(src[1], src[2]))
+    raise ValueError(kind)
+
+
+def run_reference(prog, edge_path, work):
+    empty = os.path.join(work, "empty_rel")
+    P.datagen.write_empty_relation(empty)
+    out = os.path.join(work, "out")
+    subprocess.run([DRIVER, prog, edge_path, empty, out], check=True, stdout=subprocess.DEVNULL)
+    hist = []
+    for line in open(os.path.join(out, "history.txt")):
+        a = line.split()
+        if a[0] == "scc":
+            hist.append([int(a[1]), []])
+        else:
+            hist[-1][1].append([int(a[0]), int(a[1])])
+    rels = {}
+    for line in open(os.path.join(out, "sizes.txt")):
+        name, arity, count = line.split()
+        arity, count = int(arity), int(count)
+        rows = np.fromfile(os.path.join(out, name + ".bin"), dtype="<u8").reshape(-1, arity + 1)
+        assert rows.shape[0] == count, (name, rows.shape, count)
+        rels[name] = {"arity": arity, "count": count, "sha256": rows_digest(rows)}
+        if count <= VERBATIM_MAX_ROWS:
+            rels[name]["rows"] = rows.tolist()
+    return hist, rels
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}", "-j8"], check=True)
+    for name in ("g5955", "g13236"):
+        dst = os.path.join(HERE, f"{name}_edge_2_1_2")
+        shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2"), dst)
+        shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2.size"), dst + ".size")
+    manifest = {}
+    for name, prog, src in CASES:
+        with tempfile.TemporaryDirectory() as work:
+            rows = input_rows(src, args.ref)
+            edge = os.path.join(work, "edge")
+            P.datagen.write_relation(edge, rows)
+            hist, rels = run_reference(prog, edge, work)
+        case = {"program": prog, "source": list(src), "input_rows": int(rows.shape[0]),
+                "input_sha256": rows_digest(rows), "history": hist, "relations": rels}
+        with open(os.path.join(HERE, f"{name}.json"), "w") as f:
+            json.dump(case, f, separators=(",", ":"))
+        manifest[name] = {k: case[k] for k in ("program", "source", "input_rows")}
+        print(name, {r: v["count"] for r, v in rels.items()}, "iterations", [len(h[1]) for h in hist])
+    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
