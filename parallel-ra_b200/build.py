@@ -54,9 +54,38 @@ def build_cxx(force=False):
               f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN"])
 
 
+REFERENCE = os.environ.get("RA_REFERENCE", "/root/reference")
+BIN_DIR = os.path.join(CXX_DIR, "bin")
+
+
+def build_reference_programs(force=False):
+    """Compile the reference's own program sources, unchanged, against cxx/src.
+
+    A reference program includes "../src/parallel_RA_inc.h".  The source is fed
+    to g++ on stdin from cxx/tests/, so that include resolves to
+    cxx/src/parallel_RA_inc.h; nothing is copied.  Only possible where the
+    reference tree exists; the binaries in cxx/bin/ are used elsewhere.
+    """
+    progs = {"TC": os.path.join(REFERENCE, "tests", "transitive_closure.cpp")}
+    os.makedirs(os.path.join(CXX_DIR, "tests"), exist_ok=True)
+    os.makedirs(BIN_DIR, exist_ok=True)
+    for name, src in progs.items():
+        out = os.path.join(BIN_DIR, name)
+        if not os.path.exists(src):
+            continue
+        if not (force or _stale(out, [src, CXX_LIB, os.path.join(CXX_DIR, "src", "parallel_RA_inc.h")])):
+            continue
+        cmd = ["g++", "-std=c++17", "-O2", "-x", "c++", "-", "-x", "none", "-o", out, "-L", HERE,
+               "-lparallel_ra", "-lra_b200", f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN/../.."]
+        print(" ".join(cmd), "<", src, flush=True)
+        with open(src, "rb") as f:
+            subprocess.run(cmd, check=True, stdin=f, cwd=os.path.join(CXX_DIR, "tests"))
+
+
 def build(force=False):
     build_engine(force)
     build_cxx(force)
+    build_reference_programs(force)
 
 
 if __name__ == "__main__":

@@ -69,6 +69,11 @@ struct Relation {
     // loaded rows (arity + 1 u64 each), kept on the device for reset
     u64* raw = nullptr;
     u64 raw_n = 0;
+    // packed, sorted, distinct loaded tuples (restored by reset without repacking)
+    u64* lkeys = nullptr;
+    u64* lids = nullptr;
+    u64 l_n = 0, l_cap = 0;
+    bool l_keys_unique = true;
     // log [ full | delta | newt ]
     u64* keys = nullptr;
     u64* ids = nullptr;
@@ -106,7 +111,10 @@ struct ra_program {
     std::vector<uint64_t> history;
     std::vector<std::pair<uint32_t, u64>> intern;   // (tag, next counter) -- LIE::intern_map
     int bits = 0;                 // packed bits per column for this run
+    bool packed = false;          // loaded relations packed with `bits` (cleared by a new load)
     bool executed = false;
+    bool running = false;         // between the first and the last SCC of a run
+    double fixpoint_ms_acc = 0;
     u64 epoch = 0;
     std::string err;
     ra_stats stats{};
@@ -344,6 +352,33 @@ void pack_relation(ra_program* p, Relation& r)
         r.delta_n = n;
     } else {
         r.full_n = n;
+        r.full_runs = 1;
+    }
+    grow2(p, &r.lkeys, &r.lids, &r.l_cap, n, false, 0);
+    if (n) {
+        CK(cudaMemcpyAsync(r.lkeys, r.keys, n * 8, cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(r.lids, r.ids, n * 8, cudaMemcpyDeviceToDevice, p->stream));
+    }
+    r.l_n = n;
+    r.l_keys_unique = r.keys_unique;
+}
+
+// back to the loaded tuples packed by pack_relation (same column width)
+void restore_loaded(ra_program* p, Relation& r)
+{
+    r.full_n = r.delta_n = r.newt_n = 0;
+    r.full_runs = 0;
+    r.keys_unique = r.l_keys_unique;
+    r.full_version++;
+    r.delta_version++;
+    if (!r.l_n) return;
+    ensure_log(p, r, r.l_n);
+    CK(cudaMemcpyAsync(r.keys, r.lkeys, r.l_n * 8, cudaMemcpyDeviceToDevice, p->stream));
+    CK(cudaMemcpyAsync(r.ids, r.lids, r.l_n * 8, cudaMemcpyDeviceToDevice, p->stream));
+    if (r.version == RA_DELTA) {
+        r.delta_n = r.l_n;
+    } else {
+        r.full_n = r.l_n;
         r.full_runs = 1;
     }
 }
@@ -787,39 +822,47 @@ void reset_state(ra_program* p)
     p->history.clear();
     p->intern.clear();
     p->executed = false;
+    p->running = false;
     p->epoch = 0;
 }
 
-void execute(ra_program* p)
+void begin_run(ra_program* p)
 {
-    if (p->executed) reset_state(p);
+    if (p->executed || p->running) reset_state(p);
     p->stats = ra_stats{};
     for (auto& e : p->dedup_events) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
     p->dedup_events.clear();
-    choose_bits(p);
-    for (Relation& r : p->rels) pack_relation(p, r);
-    CK(cudaEventRecord(p->ev0, p->stream));
-    for (;;) {
-        int next = -1;
-        for (size_t i = 0; i < p->sccs.size() && next < 0; i++) {
-            if (p->sccs[i].done) continue;
-            bool blocked = false;
-            for (auto& d : p->deps)
-                if (d.second == (int)i && !p->sccs[d.first].done) blocked = true;
-            if (!blocked) next = (int)i;
-        }
-        if (next < 0) break;
-        run_scc(p, p->sccs[next]);
-        p->sccs[next].done = true;
+    if (!p->packed) {
+        choose_bits(p);
+        for (Relation& r : p->rels) pack_relation(p, r);
+        p->packed = true;
+    } else {
+        for (Relation& r : p->rels) restore_loaded(p, r);
     }
-    CK(cudaEventRecord(p->ev1, p->stream));
+    p->running = true;
+    p->fixpoint_ms_acc = 0;
+}
+
+// LIE::one_runnable_tasks (src/lie/lie.cpp:27-60): first SCC, in add order, that
+// is not the destination of a dependency edge whose source has not run.
+int next_runnable(ra_program* p)
+{
+    for (size_t i = 0; i < p->sccs.size(); i++) {
+        if (p->sccs[i].done) continue;
+        bool blocked = false;
+        for (auto& d : p->deps)
+            if (d.second == (int)i && !p->sccs[d.first].done) blocked = true;
+        if (!blocked) return (int)i;
+    }
+    return -1;
+}
+
+void finish_run(ra_program* p)
+{
     CK(cudaStreamSynchronize(p->stream));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, p->ev0, p->ev1);
-    p->stats.fixpoint_ms = ms;
     double dms = 0;
     for (auto& e : p->dedup_events) {
         float m = 0;
@@ -827,8 +870,38 @@ void execute(ra_program* p)
         dms += m;
     }
     p->stats.dedup_ms = dms;
+    p->stats.fixpoint_ms = p->fixpoint_ms_acc;
     p->stats.value_bits = (uint32_t)p->bits;
     p->executed = true;
+    p->running = false;
+}
+
+// returns the SCC id that ran, or -1 when none is left (finishing the run)
+int step(ra_program* p)
+{
+    if (!p->running) begin_run(p);
+    int next = next_runnable(p);
+    if (next < 0) {
+        finish_run(p);
+        return -1;
+    }
+    CK(cudaEventRecord(p->ev0, p->stream));
+    run_scc(p, p->sccs[next]);
+    p->sccs[next].done = true;
+    CK(cudaEventRecord(p->ev1, p->stream));
+    CK(cudaEventSynchronize(p->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+    p->fixpoint_ms_acc += ms;
+    if (next_runnable(p) < 0) finish_run(p);
+    return p->sccs[next].id;
+}
+
+void execute(ra_program* p)
+{
+    if (p->executed || p->running) reset_state(p);
+    while (step(p) != -1 && p->running) {}
+    if (p->running) finish_run(p);
 }
 
 }  // namespace
@@ -895,6 +968,8 @@ int ra_program_destroy(ra_program* p)
     for (Relation& r : p->rels) {
         free_relation_state(p, r);
         dev_free(p, &r.raw);
+        dev_free(p, &r.lkeys);
+        dev_free(p, &r.lids);
     }
     dev_free(p, &p->cand);
     dev_free(p, &p->flag);
@@ -967,6 +1042,7 @@ int ra_relation_create(ra_program* p, uint32_t jcc, uint32_t arity, uint32_t tag
 
 static void set_raw(ra_program* p, Relation& r, const uint64_t* rows, uint64_t nrows, cudaMemcpyKind kind)
 {
+    p->packed = false;
     dev_free(p, &r.raw);
     r.raw_n = nrows;
     dev_alloc(p, &r.raw, nrows * (r.arity + 1));
@@ -1089,6 +1165,15 @@ int ra_scc_depend(ra_program* p, int src_scc, int dst_scc)
 int ra_program_execute(ra_program* p)
 {
     return guard(p, [&] { execute(p); });
+}
+
+int ra_program_run_next_scc(ra_program* p, int* scc_id)
+{
+    return guard(p, [&] {
+        int id = -1;
+        if (!(p->executed && !p->running)) id = step(p);
+        if (scc_id) *scc_id = id;
+    });
 }
 
 int ra_program_reset(ra_program* p)

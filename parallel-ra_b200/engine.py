@@ -23,7 +23,7 @@ EXPORTS = (
     "ra_program_create", "ra_program_destroy", "ra_program_set_stream", "ra_program_set_batch_size",
     "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
-    "ra_program_execute", "ra_program_reset", "ra_program_history", "ra_program_stats",
+    "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats",
     "ra_relation_counts", "ra_relation_dump_full", "ra_status_string", "ra_last_error",
 )
 
@@ -70,6 +70,7 @@ def lib():
         L.ra_scc_add_copy.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, i32p, C.c_int, C.c_int]
         L.ra_scc_depend.argtypes = [P, C.c_int, C.c_int]
         L.ra_program_execute.argtypes = [P]
+        L.ra_program_run_next_scc.argtypes = [P, i32p]
         L.ra_program_reset.argtypes = [P]
         L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
