@@ -59,6 +59,20 @@ typedef enum ra_status {
 #define RA_PRED_LE 6
 #define RA_PRED_GE 7
 
+/* Intern-id numbering of derived tuples (ra_program_set_id_order).  Ids are
+ * (tag << 46) | counter, counter per intern tag, as in RAM::local_insert_in_newt
+ * (src/RAM/RA_tasks.cpp:861-875).  The order in which new tuples take counter
+ * values:
+ *   RA_IDS_EMISSION  -- this engine's deterministic candidate order (default;
+ *                       deltas are not kept sorted between iterations);
+ *   RA_IDS_REFERENCE -- the single-rank reference's order: every new delta is
+ *                       radix-sorted into trie order so the next iteration
+ *                       enumerates candidates exactly as the reference does.
+ * Relation contents on the data columns and every per-iteration delta size
+ * are identical in both modes; only the id column differs. */
+#define RA_IDS_EMISSION 0
+#define RA_IDS_REFERENCE 1
+
 typedef struct ra_program ra_program;
 
 /* Per-run statistics of the last ra_program_execute. */
@@ -73,6 +87,14 @@ typedef struct ra_stats {
     uint64_t dedup_bytes;       /* algorithmic bytes moved by those kernels */
     uint32_t value_bits;        /* bits per packed column chosen for the run */
     uint32_t reserved;
+    /* Device time per phase of the device-driven iterations, filled only when
+     * the program runs with per-launch events (RA_KERNEL_EVENTS=1; no graph):
+     * [0] join scan, [1] plan, [2] expand + claim, [3] select, [4] sort,
+     * [5] iteration end. */
+    double phase_ms[6];
+    uint64_t graph_builds;      /* CUDA graphs captured + instantiated by the run */
+    double graph_build_ms;      /* host time spent building them */
+    uint64_t regrows;           /* buffer regrowths (iteration retried) */
 } ra_stats;
 
 /* Create a program on CUDA device `device`.  Replaces the per-rank set-up of
@@ -83,6 +105,9 @@ int ra_program_destroy(ra_program* p);
 int ra_program_set_stream(ra_program* p, void* stream);
 /* Iterations per fixed-point check, LIE::set_batch_size (src/lie/lie.h:111). */
 int ra_program_set_batch_size(ra_program* p, uint32_t batch_size);
+/* RA_IDS_EMISSION or RA_IDS_REFERENCE (no counterpart in the reference, whose
+ * ids depend on its rank count). */
+int ra_program_set_id_order(ra_program* p, int mode);
 
 /* relation(jcc, is_canonical, arity, tag, name, file, version),
  * src/relation/balanced_hash_relation.h:97.  arity <= 8. */

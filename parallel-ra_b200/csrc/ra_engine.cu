@@ -16,12 +16,14 @@
 //   * RAM::check_for_fixed_point's MPI_Allreduce (RA_tasks.cpp:1072-1085):
 //     device counters.
 #include "../../include/ra_engine.h"
-#include "ra_kernels.cuh"
+#include "ra_iter.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <functional>
 #include <string>
 #include <vector>
@@ -45,6 +47,10 @@ struct ra_error {
     int status;
 };
 
+// process-wide unique version stamps (caches are keyed by them)
+std::atomic<unsigned long long> g_stamp{0};
+u64 fresh_stamp() { return ++g_stamp; }
+
 struct Rule {
     int kind;            // 3 = join, else RA_COPY / RA_ACOPY / RA_COPY_FILTER
     int out, in0, ver0, in1, ver1;
@@ -60,6 +66,11 @@ struct Scc {
     std::vector<bool> init;
     std::vector<Rule> rules;
     bool done = false;
+    // instantiated fixed-point graph, reused while everything it captured is unchanged
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> graph_sig;
+    int graph_kernels = 0;
 };
 
 struct Relation {
@@ -74,18 +85,21 @@ struct Relation {
     u64* lids = nullptr;
     u64 l_n = 0, l_cap = 0;
     bool l_keys_unique = true;
+    u64 l_full_stamp = 0, l_delta_stamp = 0;   // stamps of the packed loaded state
+    bool seen_dirty = false;                    // seen set holds a previous run's keys
     // log [ full | delta | newt ]
     u64* keys = nullptr;
     u64* ids = nullptr;
     u64 cap = 0;
     u64 full_n = 0, delta_n = 0;
-    int full_runs = 0;          // sorted runs making up the full region
+    bool full_sorted = true;    // full region in trie order (lexicographic on (key, id))
+    bool delta_sorted = true;   // delta region in trie order
     bool keys_unique = true;    // no two stored tuples share data columns
     u64 full_version = 0, delta_version = 0;
     // seen set over data columns
     Slot* seen = nullptr;
     u64 seen_cap = 0, seen_n = 0;
-    // sorted view of full (used when full_runs > 1)
+    // sorted view of full (used when the full region is not sorted)
     u64* vkeys = nullptr;
     u64* vids = nullptr;
     u64 v_cap = 0, v_version = ~0ull;
@@ -105,6 +119,7 @@ struct ra_program {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     uint32_t batch_size = 1;
+    int id_order = RA_IDS_EMISSION;
     std::vector<Relation> rels;
     std::vector<Scc> sccs;
     std::vector<std::pair<int, int>> deps;
@@ -141,7 +156,27 @@ struct ra_program {
     u64* hist_off = nullptr;
     u64 hist_cap = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> dedup_events;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> phase_events;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // device-driven SCC runs (graph mode)
+    IterCtl* ctl = nullptr;
+    IterCtl* hctl = nullptr;      // pinned mirror (header part)
+    u64* dcand = nullptr;
+    u64 dcand_cap = 0;
+    u64* doff[kMaxSccRules] = {};
+    u64* dstart[kMaxSccRules] = {};
+    u64 doff_cap = 0;
+    u64* stage_k[kMaxSccRels] = {};
+    u64* stage_v[kMaxSccRels] = {};
+    u64 stage_cap = 0;
+    u64* sort_k[2] = {};
+    u64* sort_v[2] = {};
+    u64* status = nullptr;
+    u64 status_cap = 0;
+    u64* dhist = nullptr;
+    u64 dhist_cap = 0;
+    bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
+    bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
 
 namespace {
@@ -316,10 +351,10 @@ void ensure_log(ra_program* p, Relation& r, u64 n)
 void pack_relation(ra_program* p, Relation& r)
 {
     r.full_n = r.delta_n = r.newt_n = 0;
-    r.full_runs = 0;
+    r.full_sorted = r.delta_sorted = true;
     r.keys_unique = true;
-    r.full_version++;
-    r.delta_version++;
+    r.full_version = fresh_stamp();
+    r.delta_version = fresh_stamp();
     if (r.raw_n == 0) return;
     ensure_log(p, r, r.raw_n);
     rows_pack<<<grid_for(r.raw_n), kThreads, 0, p->stream>>>(r.raw, r.raw_n, (int)r.arity, p->bits, r.keys, r.ids);
@@ -348,12 +383,8 @@ void pack_relation(ra_program* p, Relation& r)
         CK(cudaMemcpyAsync(r.ids, p->tv, m * 8, cudaMemcpyDeviceToDevice, p->stream));
         n = m;
     }
-    if (r.version == RA_DELTA) {
-        r.delta_n = n;
-    } else {
-        r.full_n = n;
-        r.full_runs = 1;
-    }
+    if (r.version == RA_DELTA) r.delta_n = n;
+    else r.full_n = n;
     grow2(p, &r.lkeys, &r.lids, &r.l_cap, n, false, 0);
     if (n) {
         CK(cudaMemcpyAsync(r.lkeys, r.keys, n * 8, cudaMemcpyDeviceToDevice, p->stream));
@@ -361,38 +392,44 @@ void pack_relation(ra_program* p, Relation& r)
     }
     r.l_n = n;
     r.l_keys_unique = r.keys_unique;
+    r.l_full_stamp = r.full_version;
+    r.l_delta_stamp = r.delta_version;
 }
 
 // back to the loaded tuples packed by pack_relation (same column width)
 void restore_loaded(ra_program* p, Relation& r)
 {
     r.full_n = r.delta_n = r.newt_n = 0;
-    r.full_runs = 0;
+    r.full_sorted = r.delta_sorted = true;
     r.keys_unique = r.l_keys_unique;
-    r.full_version++;
-    r.delta_version++;
+    // same content as when packed: caches built on the loaded state stay valid
+    r.full_version = r.l_full_stamp;
+    r.delta_version = r.l_delta_stamp;
     if (!r.l_n) return;
     ensure_log(p, r, r.l_n);
     CK(cudaMemcpyAsync(r.keys, r.lkeys, r.l_n * 8, cudaMemcpyDeviceToDevice, p->stream));
     CK(cudaMemcpyAsync(r.ids, r.lids, r.l_n * 8, cudaMemcpyDeviceToDevice, p->stream));
-    if (r.version == RA_DELTA) {
-        r.delta_n = r.l_n;
-    } else {
-        r.full_n = r.l_n;
-        r.full_runs = 1;
-    }
+    if (r.version == RA_DELTA) r.delta_n = r.l_n;
+    else r.full_n = r.l_n;
 }
 
-// sorted (key, id) rows of a relation version; FULL may need a sorted copy
-void version_rows(ra_program* p, Relation& r, int ver, const u64** k, const u64** v, u64* n)
+// (key, id) rows of a relation version.  FULL rows are always returned in trie
+// order (a sorted copy when the region is not sorted); DELTA rows are sorted in
+// place when `sorted` is requested.
+void version_rows(ra_program* p, Relation& r, int ver, const u64** k, const u64** v, u64* n, bool sorted = true)
 {
     if (ver == RA_DELTA) {
+        if (sorted && !r.delta_sorted && r.delta_n > 1) {
+            sort_rows(p, r, r.keys + r.full_n, r.ids + r.full_n, r.delta_n, r.keys_unique);
+            r.delta_version = fresh_stamp();
+        }
+        if (sorted) r.delta_sorted = true;
         *k = r.keys + r.full_n;
         *v = r.ids + r.full_n;
         *n = r.delta_n;
         return;
     }
-    if (r.full_runs <= 1) {
+    if (r.full_sorted) {
         *k = r.keys;
         *v = r.ids;
         *n = r.full_n;
@@ -443,11 +480,15 @@ void build_seen(ra_program* p, Relation& r, u64 need)
 {
     u64 want = 1024;
     while (want < 2 * need) want <<= 1;
-    if (r.seen && r.seen_cap >= want) return;
-    dev_free(p, &r.seen);
-    dev_alloc(p, &r.seen, want);
+    if (r.seen && r.seen_cap >= want && !r.seen_dirty) return;
+    if (!r.seen || r.seen_cap < want) {
+        dev_free(p, &r.seen);
+        dev_alloc(p, &r.seen, want);
+        r.seen_cap = want;
+    }
+    want = r.seen_cap;
+    r.seen_dirty = false;
     CK(cudaMemsetAsync(r.seen, 0xff, want * sizeof(Slot), p->stream));
-    r.seen_cap = want;
     u64 n = r.full_n + r.delta_n;   // every stored tuple; newt is empty between iterations
     CK(cudaMemsetAsync(p->derr, 0, 4, p->stream));
     if (n) {
@@ -555,24 +596,28 @@ JoinPlan make_join_plan(ra_program* p, const Rule& ru)
 void full_to_delta(ra_program* p, Relation& r)
 {
     u64 n = r.full_n + r.delta_n;
-    bool sorted = (r.delta_n == 0 && r.full_runs <= 1) || (r.full_n == 0);
-    if (!sorted && n) sort_rows(p, r, r.keys, r.ids, n, r.keys_unique);
+    bool sorted = (r.delta_n == 0 && r.full_sorted) || (r.full_n == 0 && r.delta_sorted);
+    if (!sorted && n && p->id_order == RA_IDS_REFERENCE) {
+        sort_rows(p, r, r.keys, r.ids, n, r.keys_unique);
+        sorted = true;
+    }
     r.full_n = 0;
-    r.full_runs = 0;
+    r.full_sorted = true;
+    r.delta_sorted = sorted || n <= 1;
     r.delta_n = n;
-    r.full_version++;
-    r.delta_version++;
+    r.full_version = fresh_stamp();
+    r.delta_version = fresh_stamp();
 }
 
 // relation::insert_delta_in_full (balanced_hash_relation.cpp:1120-1148)
 void delta_to_full(Relation& r)
 {
     if (r.delta_n) {
-        r.full_runs += 1;
+        r.full_sorted = (r.full_n == 0) ? r.delta_sorted : false;
         r.full_n += r.delta_n;
         r.delta_n = 0;
-        r.full_version++;
-        r.delta_version++;
+        r.full_version = fresh_stamp();
+        r.delta_version = fresh_stamp();
     }
 }
 
@@ -603,7 +648,7 @@ void iterate(ra_program* p, Scc& s)
             Relation& in = p->rels[plans[r].inner_rel];
             const u64 *ok, *ov, *ik, *iv;
             u64 on, inn;
-            version_rows(p, o, plans[r].outer_ver, &ok, &ov, &on);
+            version_rows(p, o, plans[r].outer_ver, &ok, &ov, &on, p->id_order == RA_IDS_REFERENCE);
             version_rows(p, in, plans[r].inner_ver, &ik, &iv, &inn);
             in_keys[r] = ok;
             in_n[r] = on;
@@ -645,7 +690,7 @@ void iterate(ra_program* p, Scc& s)
                 fail(p, RA_E_UNSUPPORTED, "copy_filter on %s: predicate needs two data columns", in.name.c_str());
             const u64 *k, *v;
             u64 n;
-            version_rows(p, in, ru.ver0, &k, &v, &n);
+            version_rows(p, in, ru.ver0, &k, &v, &n, p->id_order == RA_IDS_REFERENCE);
             c[r] = n;
             if (total + n > p->cand_cap) {
                 u64 nc = (total + n) * 3 / 2 + 1024;
@@ -733,7 +778,7 @@ void iterate(ra_program* p, Scc& s)
     //    (RAM::local_insert_in_full -> insert_delta_in_full + local_insert_in_delta)
     for (int ri : s.rels) {
         Relation& r = p->rels[ri];
-        if (r.newt_n > 1) {
+        if (r.newt_n > 1 && p->id_order == RA_IDS_REFERENCE) {
             u64* nk = r.keys + r.full_n + r.delta_n;
             u64* nv = r.ids + r.full_n + r.delta_n;
             radix_sort(p, nk, nv, r.newt_n, 0, key_bits(p, r));
@@ -745,9 +790,515 @@ void iterate(ra_program* p, Scc& s)
         delta_to_full(r);
         r.delta_n = r.newt_n;
         r.newt_n = 0;
-        r.delta_version++;
+        r.delta_sorted = p->id_order == RA_IDS_REFERENCE || r.delta_n <= 1;
+        r.delta_version = fresh_stamp();
     }
     p->stats.iterations++;
+}
+
+
+// ===========================================================================
+// Device-driven SCC execution (CUDA graph with a WHILE conditional node)
+// ===========================================================================
+struct DevRule {
+    int kind;
+    int out_slot;
+    RowsRef in;            // join: outer rows; copy: input rows
+    Projection pj;
+    const u64* csr = nullptr;
+    const u64* inner = nullptr;
+    int outer_shift = 0;
+    int pred = 0;
+};
+
+struct DevScc {
+    SccPlan plan;
+    SccRelMap rm;
+    std::vector<DevRule> rules;
+    std::vector<int> rel_of_slot;   // slot -> program relation index
+    std::vector<uint32_t> tags;     // tag slot -> tag
+    int passes[kMaxSccRels];
+};
+
+size_t ctl_header_bytes() { return offsetof(IterCtl, sort_hist); }
+
+int grid_persistent() { return kSms * 4; }
+
+// Can SCC s run without host work between iterations?  Every rule must read
+// rows that either are the DELTA of one of the SCC's relations (tracked on the
+// device) or do not change while the SCC runs.
+bool build_dev_scc(ra_program* p, Scc& s, DevScc& d)
+{
+    if (s.rels.size() > (size_t)kMaxSccRels || s.rules.size() > (size_t)kMaxSccRules) return false;
+    auto slot_of = [&](int rel) {
+        for (size_t i = 0; i < s.rels.size(); i++)
+            if (s.rels[i] == rel) return (int)i;
+        return -1;
+    };
+    auto written = [&](int rel) {
+        for (const Rule& ru : s.rules)
+            if (ru.out == rel) return true;
+        return false;
+    };
+    auto static_full = [&](int rel) {
+        return !written(rel) && (slot_of(rel) < 0 || p->rels[rel].delta_n == 0);
+    };
+    // fixed rows of (rel, ver), or slot-tracked delta
+    auto rows_ref = [&](int rel, int ver, RowsRef& out) -> bool {
+        Relation& r = p->rels[rel];
+        if (ver == RA_DELTA) {
+            int sl = slot_of(rel);
+            if (sl >= 0) {
+                out = RowsRef{r.keys, sl, 0};
+                return true;
+            }
+            out = RowsRef{r.keys + r.full_n, -1, r.delta_n};
+            return true;
+        }
+        if (!static_full(rel)) return false;
+        const u64 *k, *v;
+        u64 n;
+        version_rows(p, r, RA_FULL, &k, &v, &n);
+        out = RowsRef{k, -1, n};
+        return true;
+    };
+    d = DevScc{};
+    SccPlan& pl = d.plan;
+    pl.n_rels = (int)s.rels.size();
+    pl.n_rules = (int)s.rules.size();
+    pl.fixpoint = s.fixpoint ? 1 : 0;
+    pl.batch_size = p->batch_size;
+    pl.iter_limit = 1ull << 40;
+    for (int ri : s.rels) d.rel_of_slot.push_back(ri);
+    for (size_t i = 0; i < s.rels.size(); i++) {
+        Relation& r = p->rels[s.rels[i]];
+        pl.rel_tag_word[i] = (u64)r.tag << 46;
+        d.passes[i] = std::max(1, (key_bits(p, r) + kRadixBits - 1) / kRadixBits);
+        if (d.passes[i] > kMaxPasses) return false;
+    }
+    for (size_t q = 0; q < s.rules.size(); q++) {
+        const Rule& ru = s.rules[q];
+        DevRule dr;
+        dr.kind = ru.kind;
+        dr.out_slot = slot_of(ru.out);
+        if (dr.out_slot < 0) return false;
+        uint32_t tag = p->rels[ru.out].tag;
+        int ts = -1;
+        for (size_t t = 0; t < d.tags.size(); t++)
+            if (d.tags[t] == tag) ts = (int)t;
+        if (ts < 0) {
+            if (d.tags.size() >= (size_t)kMaxTagSlots) return false;
+            d.tags.push_back(tag);
+            ts = (int)d.tags.size() - 1;
+        }
+        pl.rule_out[q] = dr.out_slot;
+        pl.rule_tag[q] = ts;
+        if (ru.kind == kJoin) {
+            JoinPlan jp = make_join_plan(p, ru);
+            // the inner side must not change while the SCC runs
+            if (jp.inner_ver == RA_FULL ? !static_full(jp.inner_rel) : slot_of(jp.inner_rel) >= 0) return false;
+            if (!rows_ref(jp.outer_rel, jp.outer_ver, dr.in)) return false;
+            Relation& in = p->rels[jp.inner_rel];
+            const u64 *ik, *iv;
+            u64 inn;
+            version_rows(p, in, jp.inner_ver, &ik, &iv, &inn);
+            dr.inner = ik;
+            dr.csr = version_csr(p, in, jp.inner_ver);
+            dr.pj = jp.pj;
+            const Relation& o = p->rels[jp.outer_rel];
+            dr.outer_shift = (int)(o.arity - o.jcc) * p->bits;
+            pl.rule_is_join[q] = 1;
+            pl.rule_in_slot[q] = -1;
+        } else {
+            if (ru.kind == RA_ACOPY) return false;
+            Relation& in = p->rels[ru.in0];
+            dr.pj = make_copy_proj(p, ru, in, p->rels[ru.out]);
+            if (ru.kind == RA_COPY_FILTER && ru.pred >= 2 && in.arity < 2)
+                fail(p, RA_E_UNSUPPORTED, "copy_filter on %s: predicate needs two data columns", in.name.c_str());
+            dr.pred = ru.kind == RA_COPY_FILTER ? ru.pred : 0;
+            if (!rows_ref(ru.in0, ru.ver0, dr.in)) return false;
+            pl.rule_is_join[q] = 0;
+            pl.rule_in_slot[q] = dr.in.slot;
+            pl.rule_in_static_n[q] = dr.in.static_n;
+        }
+        d.rules.push_back(dr);
+    }
+    for (int sl = 0; sl < pl.n_rels; sl++) {
+        d.rm.n_rules_in[sl] = 0;
+        for (int q = 0; q < pl.n_rules; q++)
+            if (pl.rule_out[q] == sl) d.rm.rules_in[sl][d.rm.n_rules_in[sl]++] = q;
+    }
+    return true;
+}
+
+// rows read from an SCC relation's DELTA follow its log, which may have moved
+void refresh_refs(ra_program* p, DevScc& d)
+{
+    for (DevRule& r : d.rules)
+        if (r.in.slot >= 0) r.in.keys = p->rels[d.rel_of_slot[r.in.slot]].keys;
+}
+
+// (Re)size every buffer the iteration touches to the plan's capacities.
+void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 off_cap, u64 stage_cap, u64 hist_cap)
+{
+    if (cand_cap > p->dcand_cap) {
+        dev_free(p, &p->dcand);
+        dev_alloc(p, &p->dcand, cand_cap);
+        p->dcand_cap = cand_cap;
+    }
+    if (off_cap > p->doff_cap) {
+        for (int q = 0; q < kMaxSccRules; q++) {
+            dev_free(p, &p->doff[q]);
+            dev_free(p, &p->dstart[q]);
+        }
+        p->doff_cap = off_cap;
+    }
+    for (int q = 0; q < (int)d.rules.size(); q++)
+        if (d.rules[q].kind == kJoin && !p->doff[q]) {
+            dev_alloc(p, &p->doff[q], p->doff_cap);
+            dev_alloc(p, &p->dstart[q], p->doff_cap);
+        }
+    const bool ref = p->id_order == RA_IDS_REFERENCE;
+    if (ref && stage_cap > p->stage_cap) {
+        for (int sl = 0; sl < kMaxSccRels; sl++) {
+            dev_free(p, &p->stage_k[sl]);
+            dev_free(p, &p->stage_v[sl]);
+        }
+        for (int b = 0; b < 2; b++) {
+            dev_free(p, &p->sort_k[b]);
+            dev_free(p, &p->sort_v[b]);
+            dev_alloc(p, &p->sort_k[b], stage_cap);
+            dev_alloc(p, &p->sort_v[b], stage_cap);
+        }
+        p->stage_cap = stage_cap;
+    }
+    for (int sl = 0; sl < d.plan.n_rels && ref; sl++)
+        if (d.rm.n_rules_in[sl] && !p->stage_k[sl]) {
+            dev_alloc(p, &p->stage_k[sl], p->stage_cap);
+            dev_alloc(p, &p->stage_v[sl], p->stage_cap);
+        }
+    u64 st_need = std::max<u64>({p->doff_cap / kScanTile + 2, p->dcand_cap / kSelTile + 2,
+                                 (p->stage_cap / kSortTile + 2) * kRadix});
+    if (st_need > p->status_cap) {
+        dev_free(p, &p->status);
+        dev_alloc(p, &p->status, st_need);
+        p->status_cap = st_need;
+    }
+    if (hist_cap > p->dhist_cap) {
+        u64* nh;
+        dev_alloc(p, &nh, 2 * hist_cap);
+        if (p->dhist) CK(cudaMemcpyAsync(nh, p->dhist, 2 * p->dhist_cap * 8, cudaMemcpyDeviceToDevice, p->stream));
+        dev_free(p, &p->dhist);
+        p->dhist = nh;
+        p->dhist_cap = hist_cap;
+    }
+    SccPlan& pl = d.plan;
+    pl.cand_cap = p->dcand_cap;
+    pl.off_cap = p->doff_cap;
+    pl.stage_cap = ref ? p->stage_cap : ~0ull;
+    pl.hist_cap = p->dhist_cap;
+    for (int sl = 0; sl < pl.n_rels; sl++) {
+        Relation& r = p->rels[d.rel_of_slot[sl]];
+        pl.log_cap[sl] = r.cap;
+        pl.seen_limit[sl] = r.seen ? (u64)(0.65 * (double)r.seen_cap) : 0;
+    }
+}
+
+// per-launch events (diagnostic mode only; never inside a graph capture)
+struct PhaseTimer {
+    ra_program* p;
+    int phase;
+    bool on;
+    PhaseTimer(ra_program* pp, int ph) : p(pp), phase(ph), on(pp->kernel_events)
+    {
+        if (!on) return;
+        cudaEvent_t a = nullptr, b = nullptr;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, p->stream);
+        p->phase_events.push_back({phase, {a, b}});
+    }
+    ~PhaseTimer()
+    {
+        if (on) cudaEventRecord(p->phase_events.back().second.second, p->stream);
+    }
+};
+
+// launches of one iteration, in order; returns the number of kernels
+int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, int use_cond)
+{
+    const SccPlan& pl = d.plan;
+    const int G = grid_persistent();
+    int launches = 0;
+    int slot = 0;
+    for (int q = 0; q < pl.n_rules; q++) {
+        const DevRule& r = d.rules[q];
+        if (r.kind != kJoin) continue;
+        PhaseTimer pt(p, 0);
+        join_scan_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, p->doff[q],
+                                                        p->dstart[q], p->doff_cap, p->status, slot++);
+        launches++;
+    }
+    {
+        PhaseTimer pt(p, 1);
+        iter_plan_kernel<<<1, 32, 0, p->stream>>>(p->ctl, pl);
+        launches++;
+    }
+    for (int q = 0; q < pl.n_rules; q++) {
+        const DevRule& r = d.rules[q];
+        Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
+        PhaseTimer pt(p, 2);
+        if (r.kind == kJoin)
+            join_insert_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, p->doff[q], p->dstart[q], r.inner, r.pj,
+                                                              p->bits, p->dcand, out.seen, out.seen_cap - 1);
+        else
+            copy_insert_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.pj, p->bits, r.pred, p->dcand,
+                                                              out.seen, out.seen_cap - 1);
+        launches++;
+    }
+    const bool ref = p->id_order == RA_IDS_REFERENCE;
+    for (int q = 0; q < pl.n_rules; q++) {
+        const DevRule& r = d.rules[q];
+        Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
+        PhaseTimer pt(p, 3);
+        select_kernel<<<G, kThreads, 0, p->stream>>>(
+            p->ctl, pl, q, p->dcand, out.seen, out.seen_cap - 1, ref ? p->stage_k[r.out_slot] : out.keys,
+            ref ? p->stage_v[r.out_slot] : out.ids, p->status, slot++, ref ? d.passes[r.out_slot] : 0, ref ? 0 : 1);
+        launches++;
+    }
+    for (int sl = 0; sl < pl.n_rels && ref; sl++) {
+        if (!d.rm.n_rules_in[sl]) continue;
+        Relation& r = p->rels[d.rel_of_slot[sl]];
+        const int P = d.passes[sl];
+        for (int ps = 0; ps < P; ps++) {
+            SortPassArgs a{};
+            a.rel = sl;
+            a.pass = ps;
+            a.shift = ps * kRadixBits;
+            a.src_k = ps == 0 ? p->stage_k[sl] : p->sort_k[(ps - 1) & 1];
+            a.src_v = ps == 0 ? p->stage_v[sl] : p->sort_v[(ps - 1) & 1];
+            a.dst_log = (ps == P - 1) ? 1 : 0;
+            a.dst_k = a.dst_log ? r.keys : p->sort_k[ps & 1];
+            a.dst_v = a.dst_log ? r.ids : p->sort_v[ps & 1];
+            a.n_rules_in = d.rm.n_rules_in[sl];
+            for (int q = 0; q < a.n_rules_in; q++) a.rules_in[q] = d.rm.rules_in[sl][q];
+            PhaseTimer pt(p, 4);
+            sort_pass_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, a, p->status, slot++);
+            launches++;
+        }
+    }
+    {
+        PhaseTimer pt(p, 5);
+        iter_end_kernel<<<64, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, p->dhist, cond, use_cond);
+        launches++;
+    }
+    ck(p, cudaGetLastError(), "iteration launch");
+    return launches;
+}
+
+// Every value an iteration's launches capture (pointers, capacities, plans).
+std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
+{
+    std::vector<unsigned char> sig;
+    auto put = [&](const void* a, size_t n) {
+        const unsigned char* b = (const unsigned char*)a;
+        sig.insert(sig.end(), b, b + n);
+    };
+    put(&d.plan, sizeof d.plan);
+    put(&d.rm, sizeof d.rm);
+    put(d.passes, sizeof d.passes);
+    for (const DevRule& r : d.rules) put(&r, sizeof r);
+    for (int sl = 0; sl < d.plan.n_rels; sl++) {
+        const Relation& r = p->rels[d.rel_of_slot[sl]];
+        const void* ptrs[4] = {r.keys, r.ids, r.seen, nullptr};
+        put(ptrs, sizeof ptrs);
+        put(&r.seen_cap, sizeof r.seen_cap);
+    }
+    const void* scratch[8] = {p->ctl, p->dcand, p->status, p->dhist, p->sort_k[0], p->sort_k[1], p->sort_v[0],
+                              p->sort_v[1]};
+    put(scratch, sizeof scratch);
+    put(p->doff, sizeof p->doff);
+    put(p->dstart, sizeof p->dstart);
+    put(p->stage_k, sizeof p->stage_k);
+    put(p->stage_v, sizeof p->stage_v);
+    put(&p->doff_cap, sizeof p->doff_cap);
+    put(&p->bits, sizeof p->bits);
+    put(&p->stream, sizeof p->stream);
+    put(&p->id_order, sizeof p->id_order);
+    return sig;
+}
+
+void drop_graph(Scc& s)
+{
+    if (s.exec) cudaGraphExecDestroy(s.exec);
+    if (s.graph) cudaGraphDestroy(s.graph);
+    s.exec = nullptr;
+    s.graph = nullptr;
+    s.graph_sig.clear();
+}
+
+void ctl_download(ra_program* p)
+{
+    CK(cudaMemcpyAsync(p->hctl, p->ctl, ctl_header_bytes(), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+}
+
+void run_scc_device(ra_program* p, Scc& s, DevScc& d)
+{
+    const SccPlan& pl = d.plan;
+    // control block: counters of the SCC's relations
+    IterCtl& h = *p->hctl;
+    std::memset(&h, 0, ctl_header_bytes());
+    std::vector<u64> full0(pl.n_rels), delta0(pl.n_rels);
+    std::vector<bool> dsorted0(pl.n_rels);
+    for (int sl = 0; sl < pl.n_rels; sl++) {
+        Relation& r = p->rels[d.rel_of_slot[sl]];
+        h.full_n[sl] = r.full_n;
+        h.delta_n[sl] = r.delta_n;
+        full0[sl] = r.full_n;
+        delta0[sl] = r.delta_n;
+        dsorted0[sl] = r.delta_sorted;
+    }
+    for (size_t t = 0; t < d.tags.size(); t++) h.intern[t] = intern_counter(p, d.tags[t]);
+    h.epoch = p->epoch + 1;
+    // seen sets of the output relations (sized with room for growth)
+    for (int sl = 0; sl < pl.n_rels; sl++) {
+        if (!d.rm.n_rules_in[sl]) continue;
+        Relation& r = p->rels[d.rel_of_slot[sl]];
+        u64 base = r.full_n + r.delta_n;
+        build_seen(p, r, std::max<u64>(2 * base, 1u << 20));
+        h.seen_n[sl] = r.seen_n;
+        ensure_log(p, r, base + std::max<u64>(base, 1u << 20));
+    }
+    refresh_refs(p, d);
+    CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemsetAsync(&p->ctl->sort_hist[0][0][0], 0, sizeof(p->ctl->sort_hist), p->stream));
+    u64 outer0 = 0;
+    for (const DevRule& r : d.rules) outer0 = std::max(outer0, r.in.slot >= 0 ? p->rels[d.rel_of_slot[r.in.slot]].delta_n : r.in.static_n);
+    dev_size_buffers(p, d, std::max<u64>({p->dcand_cap, 1u << 22, 2 * outer0}), std::max<u64>({p->doff_cap, 1u << 20, outer0}),
+                     std::max<u64>({p->stage_cap, 1u << 22, 2 * outer0}), std::max<u64>(p->dhist_cap, 1u << 12));
+    CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+
+    int body_kernels = 0;
+    const bool graph_mode = p->use_graphs && !p->kernel_events && s.fixpoint;
+    for (;;) {
+        if (graph_mode) {
+            std::vector<unsigned char> sig = graph_signature(p, d);
+            if (s.exec && sig != s.graph_sig) drop_graph(s);
+            if (!s.exec) {
+                auto gt0 = std::chrono::steady_clock::now();
+                cudaGraph_t graph = nullptr;
+                cudaGraphExec_t exec = nullptr;
+                CK(cudaGraphCreate(&graph, 0));
+                cudaGraphConditionalHandle cond;
+                CK(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+                cudaGraphNodeParams cp = {};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = cond;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                cudaGraphNode_t node;
+                CK(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                CK(cudaStreamBeginCaptureToGraph(p->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+                const int body_kernels_captured = launch_iteration(p, d, cond, 1);
+                CK(cudaStreamEndCapture(p->stream, &body));
+                CK(cudaGraphInstantiate(&exec, graph, 0));
+                s.graph = graph;
+                s.exec = exec;
+                s.graph_sig = sig;
+                body_kernels = 0;
+                p->stats.graph_builds++;
+                p->stats.graph_build_ms +=
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - gt0).count();
+                s.graph_kernels = body_kernels_captured;
+            }
+            body_kernels = s.graph_kernels;
+            CK(cudaGraphLaunch(s.exec, p->stream));
+            ctl_download(p);
+        } else {
+            // one iteration per host round trip (non-fixpoint SCCs, or graphs disabled)
+            body_kernels = launch_iteration(p, d, 0, 0);
+            ctl_download(p);
+        }
+        const u64 iters_done = h.iteration;
+        (void)iters_done;
+        if (h.flags & kFlagTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a device-side look-back wait gave up", s.id);
+        if (h.flags & kFlagProbe) fail(p, RA_E_STATE, "SCC %d: seen-set probe overflow", s.id);
+        if (h.flags & kFlagOverflow) {
+            // nothing was mutated by the overflowing iteration: grow and retry it
+            p->stats.regrows++;
+            u64 total = 0, max_outer = 0;
+            u64 incoming[kMaxSccRels] = {0};
+            for (int q = 0; q < pl.n_rules; q++) {
+                total += h.cand_n[q];
+                incoming[pl.rule_out[q]] += h.cand_n[q];
+                const RowsRef& in = d.rules[q].in;
+                max_outer = std::max(max_outer, in.slot >= 0 ? h.delta_n[in.slot] : in.static_n);
+            }
+            u64 stage_need = 0;
+            for (int sl = 0; sl < pl.n_rels; sl++) stage_need = std::max(stage_need, incoming[sl]);
+            for (int sl = 0; sl < pl.n_rels; sl++) {
+                if (!d.rm.n_rules_in[sl]) continue;
+                Relation& r = p->rels[d.rel_of_slot[sl]];
+                r.full_n = h.full_n[sl];
+                r.delta_n = h.delta_n[sl];
+                const u64 stored = r.full_n + r.delta_n;
+                if (stored + incoming[sl] > r.cap) ensure_log(p, r, 2 * (stored + incoming[sl]));
+                if (h.seen_n[sl] + incoming[sl] > (u64)(0.65 * (double)r.seen_cap)) {
+                    // rebuild from the stored tuples (all older than the retried iteration)
+                    dev_free(p, &r.seen);
+                    r.seen_cap = 0;
+                    build_seen(p, r, 4 * (stored + incoming[sl]));
+                    h.seen_n[sl] = r.seen_n;
+                }
+            }
+            refresh_refs(p, d);
+            dev_size_buffers(p, d, std::max(p->dcand_cap, 2 * total), std::max(p->doff_cap, 2 * max_outer),
+                             std::max(p->stage_cap, 2 * stage_need),
+                             h.hist_n >= p->dhist_cap ? 2 * p->dhist_cap : p->dhist_cap);
+            h.flags = 0;
+            CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
+            CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+            continue;
+        }
+        if (h.done) break;
+    }
+    // results back into the host-side relation records
+    std::vector<u64> hist(2 * h.hist_n);
+    if (h.hist_n) {
+        CK(cudaMemcpyAsync(hist.data(), p->dhist, 2 * h.hist_n * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+    }
+    for (int sl = 0; sl < pl.n_rels; sl++) {
+        Relation& r = p->rels[d.rel_of_slot[sl]];
+        if (h.full_n[sl] != r.full_n || h.delta_n[sl] != r.delta_n) {
+            const bool ref = p->id_order == RA_IDS_REFERENCE;
+            if (h.runs[sl]) {
+                // one run into an empty full keeps it sorted when that run was sorted: the SCC's
+                // initial delta, or a new delta in reference id order
+                const bool run_sorted = delta0[sl] ? dsorted0[sl] : ref;
+                r.full_sorted = full0[sl] == 0 && h.runs[sl] == 1 && run_sorted;
+            }
+            if (h.iteration) r.delta_sorted = ref || h.delta_n[sl] <= 1;
+            r.full_n = h.full_n[sl];
+            r.delta_n = h.delta_n[sl];
+            r.full_version = fresh_stamp();
+            r.delta_version = fresh_stamp();
+        }
+        if (d.rm.n_rules_in[sl]) r.seen_n = h.seen_n[sl];
+    }
+    for (size_t t = 0; t < d.tags.size(); t++) intern_counter(p, d.tags[t]) = h.intern[t];
+    p->epoch = h.epoch;
+    p->stats.iterations += h.iteration;
+    p->stats.join_candidates += h.candidates;
+    p->stats.new_tuples += h.new_tuples;
+    p->stats.kernel_launches += (u64)body_kernels * h.iteration;
+    p->stats.dedup_launches += (u64)d.rules.size() * h.iteration;
+    p->stats.dedup_bytes += 48 * h.candidates + 24 * h.outer_rows;
+    p->history.push_back((uint64_t)s.id);
+    p->history.push_back(h.hist_n);
+    p->history.insert(p->history.end(), hist.begin(), hist.end());
 }
 
 void run_scc(ra_program* p, Scc& s)
@@ -758,6 +1309,14 @@ void run_scc(ra_program* p, Scc& s)
                  p->rels[ru.out].name.c_str());
     for (size_t i = 0; i < s.rels.size(); i++)
         if (s.init[i]) full_to_delta(p, p->rels[s.rels[i]]);
+    {
+        DevScc d;
+        if (build_dev_scc(p, s, d)) {
+            run_scc_device(p, s, d);
+            for (int ri : s.rels) delta_to_full(p->rels[ri]);
+            return;
+        }
+    }
     std::vector<uint64_t> hist;
     for (;;) {
         uint32_t b = p->batch_size;
@@ -815,9 +1374,18 @@ void free_relation_state(ra_program* p, Relation& r)
     r.full_n = r.delta_n = r.newt_n = 0;
 }
 
+// Back to the pre-run state.  Device buffers are kept (capacities carry over to
+// the next run); only counters, caches of derived data and seen sets are reset.
 void reset_state(ra_program* p)
 {
-    for (Relation& r : p->rels) free_relation_state(p, r);
+    for (Relation& r : p->rels) {
+        r.full_n = r.delta_n = r.newt_n = 0;
+        r.full_sorted = r.delta_sorted = true;
+        r.seen_n = 0;
+        if (r.seen) r.seen_dirty = true;
+        r.full_version = fresh_stamp();
+        r.delta_version = fresh_stamp();
+    }
     for (Scc& s : p->sccs) s.done = false;
     p->history.clear();
     p->intern.clear();
@@ -869,6 +1437,17 @@ void finish_run(ra_program* p)
         cudaEventElapsedTime(&m, e.first, e.second);
         dms += m;
     }
+    for (auto& e : p->phase_events) {
+        float m = 0;
+        cudaEventElapsedTime(&m, e.second.first, e.second.second);
+        p->stats.phase_ms[e.first] += m;
+        if (e.first == 2) {
+            dms += m;
+        }
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    p->phase_events.clear();
     p->stats.dedup_ms = dms;
     p->stats.fixpoint_ms = p->fixpoint_ms_acc;
     p->stats.value_bits = (uint32_t)p->bits;
@@ -951,6 +1530,10 @@ int ra_program_create(int device, ra_program** out)
         CK(cudaMallocHost(&p->hscalar, 64));
         CK(cudaEventCreate(&p->ev0));
         CK(cudaEventCreate(&p->ev1));
+        dev_alloc(p, &p->ctl, 1);
+        CK(cudaMallocHost(&p->hctl, sizeof(IterCtl)));
+        if (const char* e = getenv("RA_NO_GRAPH")) p->use_graphs = atoi(e) == 0;
+        if (const char* e = getenv("RA_KERNEL_EVENTS")) p->kernel_events = atoi(e) != 0;
     });
     if (st != RA_OK) {
         delete p;
@@ -985,12 +1568,30 @@ int ra_program_destroy(ra_program* p)
     dev_free(p, &p->derr);
     dev_free(p, &p->hist_buf);
     dev_free(p, &p->hist_off);
+    dev_free(p, &p->ctl);
+    dev_free(p, &p->dcand);
+    for (int q = 0; q < kMaxSccRules; q++) {
+        dev_free(p, &p->doff[q]);
+        dev_free(p, &p->dstart[q]);
+    }
+    for (int sl = 0; sl < kMaxSccRels; sl++) {
+        dev_free(p, &p->stage_k[sl]);
+        dev_free(p, &p->stage_v[sl]);
+    }
+    for (int b = 0; b < 2; b++) {
+        dev_free(p, &p->sort_k[b]);
+        dev_free(p, &p->sort_v[b]);
+    }
+    dev_free(p, &p->status);
+    dev_free(p, &p->dhist);
+    for (Scc& sc : p->sccs) drop_graph(sc);
     for (auto& e : p->dedup_events) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
     if (p->stream) cudaStreamSynchronize(p->stream);
     if (p->hscalar) cudaFreeHost(p->hscalar);
+    if (p->hctl) cudaFreeHost(p->hctl);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
@@ -1018,6 +1619,15 @@ int ra_program_set_batch_size(ra_program* p, uint32_t batch_size)
     return guard(p, [&] {
         if (batch_size == 0) fail(p, RA_E_BADARG, "batch size must be positive");
         p->batch_size = batch_size;
+    });
+}
+
+int ra_program_set_id_order(ra_program* p, int mode)
+{
+    return guard(p, [&] {
+        if (mode != RA_IDS_REFERENCE && mode != RA_IDS_EMISSION) fail(p, RA_E_BADARG, "id order mode");
+        if (p->running) fail(p, RA_E_STATE, "id order cannot change during a run");
+        p->id_order = mode;
     });
 }
 

@@ -191,10 +191,11 @@ __global__ void __launch_bounds__(kThreads) copy_expand(const u64* __restrict__ 
 // position among equal candidates marks the first occurrence, which is the
 // tuple the reference inserts (and interns) first.
 // ---------------------------------------------------------------------------
-struct Slot {
+struct alignas(16) Slot {
     u64 key;
     u64 tag;
 };
+__device__ __forceinline__ bool slot_eq(const Slot& a, const Slot& b) { return a.key == b.key && a.tag == b.tag; }
 
 // Returns the slot holding k (inserting it if absent), or ~0 if the table is full.
 __device__ __forceinline__ u64 seen_find_or_insert(Slot* __restrict__ t, u64 mask, u64 k)

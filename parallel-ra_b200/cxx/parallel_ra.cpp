@@ -114,6 +114,10 @@ bool LIE::execute()
     int device = 0;
     if (const char* e = getenv("RA_DEVICE")) device = atoi(e);
     if (!prog) RA_CK(nullptr, ra_program_create(device, &prog));
+    /* RA_ID_ORDER=reference numbers new tuples exactly as the single-rank
+     * reference does (see ra_program_set_id_order); default: emission order */
+    if (const char* e = getenv("RA_ID_ORDER"))
+        RA_CK(prog, ra_program_set_id_order(prog, strcmp(e, "reference") == 0 ? RA_IDS_REFERENCE : RA_IDS_EMISSION));
 
     if (enable_io || restart_flag)
         fprintf(stderr, "parallel-RA (B200): checkpoint dumps and restart are not implemented; running without them\n");

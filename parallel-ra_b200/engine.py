@@ -17,10 +17,12 @@ LIB_PATH = os.path.join(HERE, "libra_b200.so")
 
 DELTA, FULL = 0, 1
 COPY, ACOPY, COPY_FILTER = 0, 1, 2
+IDS_EMISSION, IDS_REFERENCE = 0, 1
 
 # every entry point declared in include/ra_engine.h
 EXPORTS = (
     "ra_program_create", "ra_program_destroy", "ra_program_set_stream", "ra_program_set_batch_size",
+    "ra_program_set_id_order",
     "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
     "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats",
@@ -39,8 +41,10 @@ class Stats(C.Structure):
         ("iterations", C.c_uint64), ("join_candidates", C.c_uint64), ("new_tuples", C.c_uint64),
         ("kernel_launches", C.c_uint64), ("fixpoint_ms", C.c_double), ("dedup_ms", C.c_double),
         ("dedup_launches", C.c_uint64), ("dedup_bytes", C.c_uint64), ("value_bits", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("reserved", C.c_uint32), ("phase_ms", C.c_double * 6), ("graph_builds", C.c_uint64),
+        ("graph_build_ms", C.c_double), ("regrows", C.c_uint64),
     ]
+    PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 
 
 _lib = None
@@ -60,6 +64,7 @@ def lib():
         L.ra_program_destroy.argtypes = [P]
         L.ra_program_set_stream.argtypes = [P, P]
         L.ra_program_set_batch_size.argtypes = [P, C.c_uint32]
+        L.ra_program_set_id_order.argtypes = [P, C.c_int]
         L.ra_relation_create.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int, i32p]
         L.ra_relation_load_rows.argtypes = [P, C.c_int, u64p, C.c_uint64]
         L.ra_relation_load_rows_device.argtypes = [P, C.c_int, C.c_void_p, C.c_uint64]
@@ -91,7 +96,7 @@ def _u64(a: np.ndarray):
 class Program:
     """One Datalog program on one GPU (an ``ra_program``)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, id_order: int | None = None):
         self._L = lib()
         h = C.c_void_p()
         st = self._L.ra_program_create(device, C.byref(h))
@@ -99,6 +104,8 @@ class Program:
             raise RAError(st, f"ra_program_create(device={device}): {self._L.ra_status_string(st).decode()}")
         self._p = h
         self._arity = {}
+        if id_order is not None:
+            self.set_id_order(id_order)
 
     def _ck(self, st, what):
         if st != 0:
@@ -119,6 +126,10 @@ class Program:
 
     def set_stream(self, stream_ptr: int):
         self._ck(self._L.ra_program_set_stream(self._p, C.c_void_p(stream_ptr)), "set_stream")
+
+    def set_id_order(self, mode: int):
+        """IDS_EMISSION (default) or IDS_REFERENCE (single-rank reference numbering)."""
+        self._ck(self._L.ra_program_set_id_order(self._p, mode), "set_id_order")
 
     def set_batch_size(self, n: int):
         self._ck(self._L.ra_program_set_batch_size(self._p, n), "set_batch_size")

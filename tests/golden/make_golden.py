@@ -6,8 +6,9 @@ oracle/Makefile against a single-rank MPI stand-in) on
     data/g13236/edge_2_1_2 (copied here as fixtures), and
   * seeded synthetic graphs (TC on Erdos-Renyi graphs, SG on random trees),
 and records, per case, the per-SCC history of (sum |delta|, sum |full|)
-pairs, every relation's full count, and a SHA-256 of each relation's sorted
-rows (data columns + intern id).  Small relations are also stored verbatim.
+pairs, every relation's full count, a SHA-256 of each relation's sorted rows
+(data columns + intern id) and one of its data columns alone.  Small
+relations are also stored verbatim.
 
 Needs the reference tree (default /root/reference); run from the repo root:
     python tests/golden/make_golden.py [--ref /root/reference]
@@ -78,7 +79,8 @@ def run_reference(prog, edge_path, work):
         arity, count = int(arity), int(count)
         rows = np.fromfile(os.path.join(out, name + ".bin"), dtype="<u8").reshape(-1, arity + 1)
         assert rows.shape[0] == count, (name, rows.shape, count)
-        rels[name] = {"arity": arity, "count": count, "sha256": rows_digest(rows)}
+        rels[name] = {"arity": arity, "count": count, "sha256": rows_digest(rows),
+                      "data_sha256": rows_digest(rows[:, :arity])}
         if count <= VERBATIM_MAX_ROWS:
             rels[name]["rows"] = rows.tolist()
     return hist, rels
