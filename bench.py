@@ -42,11 +42,15 @@ METRIC_FAMILY = "TC tuples/s + HBM GB/s on 1 B200; batched vs serial instances/s
 WORKLOADS = {
     # name: (nodes, edges, seed)
     "tc-er22": (1 << 22, 3984589, 2),
+    "tc-er20": (1 << 20, 996147, 2),        # same family at 1/4 scale (profiling case)
     "tc-er2000": (2000, 3000, 1),
 }
 # bounded CPU sample of the same graph family (mean out-degree 0.95)
 CPU_SAMPLE = (1 << 17, round(0.95 * (1 << 17)), 2)
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per launch of join_insert_kernel from the ncu capture
+# summarised in profiles/ (None until captured for this kernel version)
+TRAFFIC_PER_LAUNCH = None
 
 
 def load_peaks():
@@ -186,7 +190,7 @@ def run_ours(args, rank, world, local_rank):
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    dedup_ms = dedup_bytes = dedup_launches = launches = 0
+    launches = 0
     torch.cuda.synchronize()
     profile_range = bool(os.environ.get("RA_PROFILE_TIMED"))   # ncu --profile-from-start off
     if profile_range:
@@ -198,11 +202,7 @@ def run_ours(args, rank, world, local_rank):
             starts[i].record(stream)
             prog.execute(1)
             ends[i].record(stream)
-            st = prog.stats()
-            dedup_ms += st.dedup_ms
-            dedup_bytes += st.dedup_bytes
-            dedup_launches += st.dedup_launches
-            launches += st.kernel_launches
+            launches += prog.stats().kernel_launches
         torch.cuda.synchronize()
     if profile_range:
         torch.cuda.profiler.stop()
@@ -220,7 +220,29 @@ def run_ours(args, rank, world, local_rank):
         tc_all = int(c.item())
     value = tc_all * args.steps / (total_ms / 1e3)
     st = prog.stats()
-    hist = prog.history()
+
+    # dominant kernel (fused join expansion + first-occurrence claim): per-launch
+    # CUDA events on the engine's stream, in an instrumented pass over the same
+    # program (the timed steps run as one CUDA graph, whose nodes events cannot split)
+    prog.set_launch_timing(True)
+    dedup_ms = dedup_bytes = dedup_launches = 0
+    phase = [0.0] * 6
+    for _ in range(max(1, min(args.steps, 3))):
+        prog.execute(1)
+        s2 = prog.stats()
+        dedup_ms += s2.dedup_ms
+        dedup_bytes += s2.dedup_bytes
+        dedup_launches += s2.dedup_launches
+        phase = [a + b for a, b in zip(phase, s2.phase_ms)]
+    prog.set_launch_timing(False)
+
+    # the same program with intern ids numbered exactly as the single-rank reference
+    prog.set_id_order(P.engine.IDS_REFERENCE)
+    ref_ms = []
+    for _ in range(3):
+        prog.execute(1)
+        ref_ms.append(prog.stats().fixpoint_ms)
+    prog.set_id_order(P.engine.IDS_EMISSION)
 
     # end to end through the C ABI from pinned host rows
     pinned = torch.from_numpy(rows.view(np.int64)).pin_memory()
@@ -244,9 +266,12 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = load_peaks()
     achieved = (dedup_bytes / dedup_launches) / ((dedup_ms / dedup_launches) / 1e3) / 1e9 if dedup_launches else 0.0
-    roofline = {"kernel": "dedup_insert", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                "bytes_model": "per candidate: 8 B candidate key read + 16 B hash slot read + 16 B slot write"}
+    roofline = {"kernel": "join_insert_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": TRAFFIC_PER_LAUNCH,
+                "launches": int(dedup_launches), "avg_launch_us": 1e3 * dedup_ms / max(dedup_launches, 1),
+                "bytes_per_launch": dedup_bytes / max(dedup_launches, 1),
+                "bytes_model": "48 B per candidate (8 B inner key read, 8 B candidate write, 16 B seen-slot read "
+                               "+ 16 B write) + 24 B per outer delta row (key, row offset, CSR start)"}
     if rank != 0:
         return None
     line = {
@@ -256,6 +281,10 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": args.workload, "nodes": n, "edges": m, "seed": WORKLOADS[args.workload][2],
                    "tc_tuples": tc, "iterations": int(st.iterations), "join_candidates": int(st.join_candidates),
                    "value_bits": int(st.value_bits), "l2": "flushed (256 MiB write) before every timed step",
+                   "id_order": "emission (default)",
+                   "value_reference_ids": tc / (statistics.median(ref_ms) / 1e3),
+                   "phase_ms_per_step": {k: v / max(1, min(args.steps, 3)) for k, v in
+                                         zip(P.engine.Stats.PHASES, phase)},
                    "parallelism": f"{world} independent instance(s), one per GPU", "metric_family": METRIC_FAMILY},
         "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
         "step_ms": step_ms,

@@ -108,6 +108,11 @@ int ra_program_set_batch_size(ra_program* p, uint32_t batch_size);
 /* RA_IDS_EMISSION or RA_IDS_REFERENCE (no counterpart in the reference, whose
  * ids depend on its rank count). */
 int ra_program_set_id_order(ra_program* p, int mode);
+/* Per-launch CUDA events around every iteration kernel (fills ra_stats.phase_ms
+ * and dedup_ms); iterations are then launched from the host instead of a CUDA
+ * graph.  A profiling aid: the reference's counterpart is the per-phase
+ * MPI_Wtime table of RAM::execute_in_batches (src/RAM/RA_tasks.cpp:1138-1253). */
+int ra_program_set_launch_timing(ra_program* p, int on);
 
 /* relation(jcc, is_canonical, arity, tag, name, file, version),
  * src/relation/balanced_hash_relation.h:97.  arity <= 8. */

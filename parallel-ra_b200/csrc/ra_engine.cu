@@ -939,25 +939,13 @@ void refresh_refs(ra_program* p, DevScc& d)
 }
 
 // (Re)size every buffer the iteration touches to the plan's capacities.
-void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 off_cap, u64 stage_cap, u64 hist_cap)
+void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64 hist_cap)
 {
     if (cand_cap > p->dcand_cap) {
         dev_free(p, &p->dcand);
         dev_alloc(p, &p->dcand, cand_cap);
         p->dcand_cap = cand_cap;
     }
-    if (off_cap > p->doff_cap) {
-        for (int q = 0; q < kMaxSccRules; q++) {
-            dev_free(p, &p->doff[q]);
-            dev_free(p, &p->dstart[q]);
-        }
-        p->doff_cap = off_cap;
-    }
-    for (int q = 0; q < (int)d.rules.size(); q++)
-        if (d.rules[q].kind == kJoin && !p->doff[q]) {
-            dev_alloc(p, &p->doff[q], p->doff_cap);
-            dev_alloc(p, &p->dstart[q], p->doff_cap);
-        }
     const bool ref = p->id_order == RA_IDS_REFERENCE;
     if (ref && stage_cap > p->stage_cap) {
         for (int sl = 0; sl < kMaxSccRels; sl++) {
@@ -977,7 +965,10 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 off_cap, u64 s
             dev_alloc(p, &p->stage_k[sl], p->stage_cap);
             dev_alloc(p, &p->stage_v[sl], p->stage_cap);
         }
-    u64 st_need = std::max<u64>({p->doff_cap / kScanTile + 2, p->dcand_cap / kSelTile + 2,
+    u64 max_outer = 0;
+    for (const DevRule& r : d.rules)
+        max_outer = std::max(max_outer, r.in.slot >= 0 ? p->dcand_cap : r.in.static_n);
+    u64 st_need = std::max<u64>({max_outer / kJRows + 2, p->dcand_cap / kSelTile + 2,
                                  (p->stage_cap / kSortTile + 2) * kRadix});
     if (st_need > p->status_cap) {
         dev_free(p, &p->status);
@@ -994,7 +985,6 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 off_cap, u64 s
     }
     SccPlan& pl = d.plan;
     pl.cand_cap = p->dcand_cap;
-    pl.off_cap = p->doff_cap;
     pl.stage_cap = ref ? p->stage_cap : ~0ull;
     pl.hist_cap = p->dhist_cap;
     for (int sl = 0; sl < pl.n_rels; sl++) {
@@ -1029,65 +1019,62 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
 {
     const SccPlan& pl = d.plan;
     const int G = grid_persistent();
+    const bool ref = p->id_order == RA_IDS_REFERENCE;
     int launches = 0;
     int slot = 0;
-    for (int q = 0; q < pl.n_rules; q++) {
-        const DevRule& r = d.rules[q];
-        if (r.kind != kJoin) continue;
-        PhaseTimer pt(p, 0);
-        join_scan_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, p->doff[q],
-                                                        p->dstart[q], p->doff_cap, p->status, slot++);
-        launches++;
-    }
-    {
-        PhaseTimer pt(p, 1);
-        iter_plan_kernel<<<1, 32, 0, p->stream>>>(p->ctl, pl);
-        launches++;
-    }
     for (int q = 0; q < pl.n_rules; q++) {
         const DevRule& r = d.rules[q];
         Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
         PhaseTimer pt(p, 2);
         if (r.kind == kJoin)
-            join_insert_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, p->doff[q], p->dstart[q], r.inner, r.pj,
-                                                              p->bits, p->dcand, out.seen, out.seen_cap - 1);
+            join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
+                                                             p->bits, p->dcand, p->dcand_cap, out.seen,
+                                                             out.seen_cap - 1, p->status, slot++);
         else
-            copy_insert_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.pj, p->bits, r.pred, p->dcand,
-                                                              out.seen, out.seen_cap - 1);
+            copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
+                                                                 p->dcand, p->dcand_cap, out.seen, out.seen_cap - 1);
         launches++;
     }
-    const bool ref = p->id_order == RA_IDS_REFERENCE;
     for (int q = 0; q < pl.n_rules; q++) {
         const DevRule& r = d.rules[q];
         Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
         PhaseTimer pt(p, 3);
-        select_kernel<<<G, kThreads, 0, p->stream>>>(
-            p->ctl, pl, q, p->dcand, out.seen, out.seen_cap - 1, ref ? p->stage_k[r.out_slot] : out.keys,
-            ref ? p->stage_v[r.out_slot] : out.ids, p->status, slot++, ref ? d.passes[r.out_slot] : 0, ref ? 0 : 1);
+        SelectArgs a{};
+        a.rule = q;
+        a.last = (!ref && q == pl.n_rules - 1) ? 1 : 0;
+        a.to_log = ref ? 0 : 1;
+        a.dst_keys = ref ? p->stage_k[r.out_slot] : out.keys;
+        a.dst_ids = ref ? p->stage_v[r.out_slot] : out.ids;
+        a.passes = ref ? d.passes[r.out_slot] : 0;
+        a.log_cap = out.cap;
+        a.stage_cap = p->stage_cap;
+        select_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, out.seen, out.seen_cap - 1,
+                                                     p->status, slot++, p->dhist, cond, use_cond);
         launches++;
     }
-    for (int sl = 0; sl < pl.n_rels && ref; sl++) {
-        if (!d.rm.n_rules_in[sl]) continue;
-        Relation& r = p->rels[d.rel_of_slot[sl]];
-        const int P = d.passes[sl];
-        for (int ps = 0; ps < P; ps++) {
-            SortPassArgs a{};
-            a.rel = sl;
-            a.pass = ps;
-            a.shift = ps * kRadixBits;
-            a.src_k = ps == 0 ? p->stage_k[sl] : p->sort_k[(ps - 1) & 1];
-            a.src_v = ps == 0 ? p->stage_v[sl] : p->sort_v[(ps - 1) & 1];
-            a.dst_log = (ps == P - 1) ? 1 : 0;
-            a.dst_k = a.dst_log ? r.keys : p->sort_k[ps & 1];
-            a.dst_v = a.dst_log ? r.ids : p->sort_v[ps & 1];
-            a.n_rules_in = d.rm.n_rules_in[sl];
-            for (int q = 0; q < a.n_rules_in; q++) a.rules_in[q] = d.rm.rules_in[sl][q];
-            PhaseTimer pt(p, 4);
-            sort_pass_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, a, p->status, slot++);
-            launches++;
+    if (ref) {
+        for (int sl = 0; sl < pl.n_rels; sl++) {
+            if (!d.rm.n_rules_in[sl]) continue;
+            Relation& r = p->rels[d.rel_of_slot[sl]];
+            const int P = d.passes[sl];
+            for (int ps = 0; ps < P; ps++) {
+                SortPassArgs a{};
+                a.rel = sl;
+                a.pass = ps;
+                a.shift = ps * kRadixBits;
+                a.src_k = ps == 0 ? p->stage_k[sl] : p->sort_k[(ps - 1) & 1];
+                a.src_v = ps == 0 ? p->stage_v[sl] : p->sort_v[(ps - 1) & 1];
+                a.dst_log = (ps == P - 1) ? 1 : 0;
+                a.dst_k = a.dst_log ? r.keys : p->sort_k[ps & 1];
+                a.dst_v = a.dst_log ? r.ids : p->sort_v[ps & 1];
+                a.log_cap = r.cap;
+                a.n_rules_in = d.rm.n_rules_in[sl];
+                for (int q = 0; q < a.n_rules_in; q++) a.rules_in[q] = d.rm.rules_in[sl][q];
+                PhaseTimer pt(p, 4);
+                sort_pass_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, a, p->status, slot++);
+                launches++;
+            }
         }
-    }
-    {
         PhaseTimer pt(p, 5);
         iter_end_kernel<<<64, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, p->dhist, cond, use_cond);
         launches++;
@@ -1113,18 +1100,18 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
         const void* ptrs[4] = {r.keys, r.ids, r.seen, nullptr};
         put(ptrs, sizeof ptrs);
         put(&r.seen_cap, sizeof r.seen_cap);
+        put(&r.cap, sizeof r.cap);
     }
     const void* scratch[8] = {p->ctl, p->dcand, p->status, p->dhist, p->sort_k[0], p->sort_k[1], p->sort_v[0],
                               p->sort_v[1]};
     put(scratch, sizeof scratch);
-    put(p->doff, sizeof p->doff);
-    put(p->dstart, sizeof p->dstart);
     put(p->stage_k, sizeof p->stage_k);
     put(p->stage_v, sizeof p->stage_v);
-    put(&p->doff_cap, sizeof p->doff_cap);
     put(&p->bits, sizeof p->bits);
     put(&p->stream, sizeof p->stream);
     put(&p->id_order, sizeof p->id_order);
+    put(&p->stage_cap, sizeof p->stage_cap);
+    put(&p->dcand_cap, sizeof p->dcand_cap);
     return sig;
 }
 
@@ -1175,7 +1162,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     CK(cudaMemsetAsync(&p->ctl->sort_hist[0][0][0], 0, sizeof(p->ctl->sort_hist), p->stream));
     u64 outer0 = 0;
     for (const DevRule& r : d.rules) outer0 = std::max(outer0, r.in.slot >= 0 ? p->rels[d.rel_of_slot[r.in.slot]].delta_n : r.in.static_n);
-    dev_size_buffers(p, d, std::max<u64>({p->dcand_cap, 1u << 22, 2 * outer0}), std::max<u64>({p->doff_cap, 1u << 20, outer0}),
+    dev_size_buffers(p, d, std::max<u64>({p->dcand_cap, 1u << 22, 2 * outer0}),
                      std::max<u64>({p->stage_cap, 1u << 22, 2 * outer0}), std::max<u64>(p->dhist_cap, 1u << 12));
     CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
 
@@ -1221,20 +1208,18 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             body_kernels = launch_iteration(p, d, 0, 0);
             ctl_download(p);
         }
-        const u64 iters_done = h.iteration;
-        (void)iters_done;
         if (h.flags & kFlagTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a device-side look-back wait gave up", s.id);
-        if (h.flags & kFlagProbe) fail(p, RA_E_STATE, "SCC %d: seen-set probe overflow", s.id);
-        if (h.flags & kFlagOverflow) {
-            // nothing was mutated by the overflowing iteration: grow and retry it
+        if (h.flags & (kFlagOverflow | kFlagProbe | kFlagGrow)) {
+            // Overflow / probe: the iteration stopped before select wrote anything and its
+            // claims are idempotent, so grow and replay it.  Grow: the iteration finished;
+            // make room in the seen sets before the next one.
+            const bool replay = (h.flags & (kFlagOverflow | kFlagProbe)) != 0;
             p->stats.regrows++;
-            u64 total = 0, max_outer = 0;
+            u64 total = 0;
             u64 incoming[kMaxSccRels] = {0};
             for (int q = 0; q < pl.n_rules; q++) {
                 total += h.cand_n[q];
                 incoming[pl.rule_out[q]] += h.cand_n[q];
-                const RowsRef& in = d.rules[q].in;
-                max_outer = std::max(max_outer, in.slot >= 0 ? h.delta_n[in.slot] : in.static_n);
             }
             u64 stage_need = 0;
             for (int sl = 0; sl < pl.n_rels; sl++) stage_need = std::max(stage_need, incoming[sl]);
@@ -1244,22 +1229,31 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 r.full_n = h.full_n[sl];
                 r.delta_n = h.delta_n[sl];
                 const u64 stored = r.full_n + r.delta_n;
-                if (stored + incoming[sl] > r.cap) ensure_log(p, r, 2 * (stored + incoming[sl]));
-                if (h.seen_n[sl] + incoming[sl] > (u64)(0.65 * (double)r.seen_cap)) {
-                    // rebuild from the stored tuples (all older than the retried iteration)
+                if (replay && stored + incoming[sl] > r.cap) ensure_log(p, r, 2 * (stored + incoming[sl]));
+                const bool tight = h.seen_n[sl] + 2 * incoming[sl] > (u64)(0.6 * (double)r.seen_cap);
+                if ((h.flags & kFlagProbe) || tight) {
+                    // rebuild from the stored tuples: every key older than the next (or replayed) iteration
+                    const u64 want = std::max<u64>(4 * (stored + incoming[sl]), 2 * r.seen_cap);
                     dev_free(p, &r.seen);
                     r.seen_cap = 0;
-                    build_seen(p, r, 4 * (stored + incoming[sl]));
+                    build_seen(p, r, want);
                     h.seen_n[sl] = r.seen_n;
                 }
             }
             refresh_refs(p, d);
-            dev_size_buffers(p, d, std::max(p->dcand_cap, 2 * total), std::max(p->doff_cap, 2 * max_outer),
-                             std::max(p->stage_cap, 2 * stage_need),
+            dev_size_buffers(p, d, replay ? std::max(p->dcand_cap, 2 * total) : p->dcand_cap,
+                             replay ? std::max(p->stage_cap, 2 * stage_need) : p->stage_cap,
                              h.hist_n >= p->dhist_cap ? 2 * p->dhist_cap : p->dhist_cap);
             h.flags = 0;
+            h.exit_ctr = 0;
+            if (replay)
+                for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
             CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
-            CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+            if (replay) {
+                CK(cudaMemsetAsync(&p->ctl->sort_hist[0][0][0], 0, sizeof(p->ctl->sort_hist), p->stream));
+                CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+            }
+            if (h.done) break;
             continue;
         }
         if (h.done) break;
@@ -1272,7 +1266,8 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     }
     for (int sl = 0; sl < pl.n_rels; sl++) {
         Relation& r = p->rels[d.rel_of_slot[sl]];
-        if (h.full_n[sl] != r.full_n || h.delta_n[sl] != r.delta_n) {
+        // compare with the counts at SCC start (a mid-SCC regrow refreshes r's counts)
+        if (h.full_n[sl] != full0[sl] || h.delta_n[sl] != delta0[sl] || h.iteration) {
             const bool ref = p->id_order == RA_IDS_REFERENCE;
             if (h.runs[sl]) {
                 // one run into an empty full keeps it sorted when that run was sorted: the SCC's
@@ -1628,6 +1623,14 @@ int ra_program_set_id_order(ra_program* p, int mode)
         if (mode != RA_IDS_REFERENCE && mode != RA_IDS_EMISSION) fail(p, RA_E_BADARG, "id order mode");
         if (p->running) fail(p, RA_E_STATE, "id order cannot change during a run");
         p->id_order = mode;
+    });
+}
+
+int ra_program_set_launch_timing(ra_program* p, int on)
+{
+    return guard(p, [&] {
+        if (p->running) fail(p, RA_E_STATE, "launch timing cannot change during a run");
+        p->kernel_events = on != 0;
     });
 }
 

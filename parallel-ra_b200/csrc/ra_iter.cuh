@@ -4,18 +4,25 @@
 // until the delta is empty (RAM::check_for_fixed_point's MPI_Allreduce,
 // src/RAM/RA_tasks.cpp:1072-1085, becomes a device flag).
 //
-// Per iteration, for an SCC whose joins read the DELTA of one relation and the
-// FULL of a relation no rule of the SCC writes:
-//   join_scan      per outer (delta) row: match count from the inner CSR, single-
-//                  pass decoupled look-back scan -> first output slot per row
-//   iter_plan      stream position base per rule, capacity guard
-//   join_insert    per candidate: merge-path row lookup, projection, candidate
-//                  written, first-occurrence claim in the output's seen set
-//   copy_insert    (copy / copy_filter rules) same for one candidate per row
-//   select         per candidate: winner test, ordered compaction (look-back),
-//                  intern ids, digit histograms for the sort
-//   sort_pass x P  onesweep LSD radix passes (8-bit digits) into the log
-//   iter_end       region bump, history, intern counters, graph condition
+// Per iteration, for an SCC whose rules read the DELTA of its relations and
+// inputs that do not change while it runs (e.g. the FULL of a loaded relation):
+//   join_fused     per tile of outer (delta) rows: match counts from the inner
+//                  CSR, single-pass decoupled look-back scan of the counts, then
+//                  the tile's candidates expanded in place (merge-path over the
+//                  tile's rows, so a heavy row is spread over all the block's
+//                  warps), written to the candidate stream and claimed in the
+//                  output relation's seen set (first occurrence = least stream
+//                  position) -- count, scan and write in one launch
+//   copy_claim     (copy / copy_filter rules) one candidate per input row
+//   select         per candidate: winner test, ordered compaction (look-back)
+//                  straight into the relation's log, intern ids; the last tile
+//                  of the last rule runs the iteration end: region bump,
+//                  history, intern counters, graph condition
+//   (reference id order only) digit histograms in select, onesweep LSD radix
+//   passes over the new delta, then a separate iteration-end launch
+// An iteration that finds a buffer too small stops before select writes
+// anything; claims made so far are idempotent, so the host grows the buffer
+// and replays the same iteration (same epoch, same stream positions).
 #pragma once
 #include "ra_kernels.cuh"
 
@@ -28,10 +35,11 @@ constexpr int kMaxPasses = 8;
 constexpr int kTileSlots = 128;
 
 // flags
-constexpr u32 kFlagOverflow = 1u;   // a buffer is too small for this iteration: nothing was mutated
-constexpr u32 kFlagTimeout = 2u;    // a bounded look-back wait gave up
-constexpr u32 kFlagProbe = 4u;      // a seen-set probe found no slot (table full)
-constexpr u32 kFlagHistory = 8u;    // history buffer full
+constexpr u32 kFlagOverflow = 1u;   // a buffer is too small: replay the iteration after growing it
+constexpr u32 kFlagTimeout = 2u;    // a bounded look-back wait gave up (fatal)
+constexpr u32 kFlagProbe = 4u;      // a seen-set probe gave up (table too full): grow, replay
+constexpr u32 kFlagGrow = 8u;       // iteration done; the seen set needs room before the next one
+constexpr u64 kMaxProbe = 4096;
 
 struct IterCtl {
     u64 full_n[kMaxSccRels], delta_n[kMaxSccRels], seen_n[kMaxSccRels];
@@ -43,7 +51,8 @@ struct IterCtl {
     u64 hist_n;             // (sum_delta, sum_full) pairs recorded
     u64 new_tuples, candidates, outer_rows;
     u64 runs[kMaxSccRels];  // non-empty deltas moved into full (sorted runs added)
-    u32 tile_ctr[kTileSlots];
+    u32 tile_ctr[2 * kTileSlots];   // two banks: iteration k uses bank k & 1
+    u32 exit_ctr;                   // blocks of the running select launch that have finished
     u32 flags;
     u32 done;
     u64 sort_hist[kMaxSccRels][kMaxPasses][kRadix];
@@ -63,7 +72,6 @@ struct SccPlan {
     u64 log_cap[kMaxSccRels];
     u64 seen_limit[kMaxSccRels];         // keys a seen set may hold
     u64 hist_cap;                        // history pairs
-    u64 off_cap;                         // per-row scan buffers (outer rows of one join)
     u64 batch_size;
     u64 iter_limit;
     int fixpoint;
@@ -191,6 +199,11 @@ __device__ __forceinline__ u32 iter_tag(const IterCtl* c, int slot)
     return (u32)(((c->iteration + 1) << 7) | (u64)slot);
 }
 
+__device__ __forceinline__ u32* tile_counter(IterCtl* c, int slot)
+{
+    return &c->tile_ctr[(c->iteration & 1) * kTileSlots + slot];
+}
+
 // first index i in [0, n) with a[i] > x (n if none)
 template <typename T>
 __device__ __forceinline__ u64 upper_bound_dev(const T* a, u64 n, u64 x)
@@ -204,124 +217,28 @@ __device__ __forceinline__ u64 upper_bound_dev(const T* a, u64 n, u64 x)
     return lo;
 }
 
-// ---------------------------------------------------------------------------
-// join_scan: count + exclusive scan in one pass
-// ---------------------------------------------------------------------------
-constexpr int kScanIpt = 4;
-constexpr int kScanTile = kThreads * kScanIpt;
-
-__global__ void __launch_bounds__(kThreads) join_scan_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
-                                                             int outer_shift, const u64* __restrict__ csr,
-                                                             u64* __restrict__ off, u64* __restrict__ start,
-                                                             u64 off_cap, u64* __restrict__ status, int tile_slot)
+// candidates of rules before `rule` in this iteration's stream
+__device__ __forceinline__ u64 stream_base(const IterCtl* c, int rule)
 {
-    __shared__ u64 sm[kWarps + 1];
-    __shared__ u32 s_tile;
-    __shared__ u64 s_prefix;
-    if (ctl->flags) return;
-    const u64 n = rows_n(ctl, outer_ref);
-    const u64* outer = rows_ptr(ctl, outer_ref);
-    const u64 ntiles = (n + kScanTile - 1) / kScanTile;
-    if (n == 0 || n > off_cap) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            ctl->cand_n[rule] = 0;
-            if (n > off_cap) atomicOr(&ctl->flags, kFlagOverflow);
-        }
-        return;
-    }
-    const u32 tag = iter_tag(ctl, tile_slot);
-    if (blockIdx.x >= ntiles) return;
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->tile_ctr[tile_slot], 1u);
-        __syncthreads();
-        const u64 tile = s_tile;
-        __syncthreads();
-        if (tile >= ntiles) break;
-        const u64 base = tile * kScanTile + (u64)threadIdx.x * kScanIpt;
-        u64 cnt[kScanIpt];
-        u64 local = 0;
-#pragma unroll
-        for (int k = 0; k < kScanIpt; k++) {
-            const u64 i = base + k;
-            cnt[k] = 0;
-            if (i < n) {
-                const u64 j = outer[i] >> outer_shift;
-                const u64 s = csr[j];
-                cnt[k] = csr[j + 1] - s;
-                start[i] = s;
-            }
-            local += cnt[k];
-        }
-        u64 agg;
-        u64 ex = block_exclusive_scan(local, sm, &agg);
-        if (threadIdx.x < 32) {
-            const u64 pre = lookback_warp(status, (u32)tile, agg, tag, &ctl->flags);
-            if (threadIdx.x == 0) s_prefix = pre;
-        }
-        __syncthreads();
-        u64 run = s_prefix + ex;
-#pragma unroll
-        for (int k = 0; k < kScanIpt; k++) {
-            const u64 i = base + k;
-            if (i < n) off[i] = run;
-            run += cnt[k];
-        }
-        if (tile == ntiles - 1 && threadIdx.x == 0) {
-            ctl->cand_n[rule] = s_prefix + agg;
-            ctl->outer_rows += n;
-        }
-        __syncthreads();
-    }
+    u64 b = 0;
+    for (int q = 0; q < rule; q++) b += c->cand_n[q];
+    return b;
 }
 
 // ---------------------------------------------------------------------------
-// iter_plan: stream bases + capacity guard (one warp)
+// first-occurrence claims: one 16-byte CAS per probed slot.  An empty slot
+// becomes {k, mine}; a slot holding k keeps the smaller tag (older tuples carry
+// tag 0).  kClaimBatch independent claims are issued back to back.
 // ---------------------------------------------------------------------------
-__global__ void iter_plan_kernel(IterCtl* __restrict__ ctl, SccPlan plan)
-{
-    if (threadIdx.x != 0 || ctl->flags) return;
-    u64 total = 0;
-    u64 incoming[kMaxSccRels] = {0};
-    for (int r = 0; r < plan.n_rules; r++) {
-        if (!plan.rule_is_join[r]) {
-            const int s = plan.rule_in_slot[r];
-            ctl->cand_n[r] = (s >= 0) ? ctl->delta_n[s] : plan.rule_in_static_n[r];
-        }
-        ctl->cand_base[r] = total;
-        total += ctl->cand_n[r];
-        incoming[plan.rule_out[r]] += ctl->cand_n[r];
-        ctl->win_n[r] = 0;
-    }
-    bool over = total > plan.cand_cap;
-    // the history entry this iteration may record must fit before anything changes
-    const bool records = !plan.fixpoint || ctl->batch_pos + 1 >= plan.batch_size;
-    over = over || (records && ctl->hist_n >= plan.hist_cap);
-    for (int s = 0; s < plan.n_rels; s++) {
-        over = over || incoming[s] > plan.stage_cap;
-        over = over || ctl->full_n[s] + ctl->delta_n[s] + incoming[s] > plan.log_cap[s];
-        over = over || ctl->seen_n[s] + incoming[s] > plan.seen_limit[s];
-    }
-    if (over) atomicOr(&ctl->flags, kFlagOverflow);
-    else ctl->candidates += total;
-}
+constexpr int kClaimBatch = 4;
 
-// ---------------------------------------------------------------------------
-// candidate expansion + first-occurrence claim
-// ---------------------------------------------------------------------------
-constexpr int kInsTile = 1024;
-constexpr int kLbsCap = 2048;
-
-// First-occurrence claim of key k by stream position `mine` (tag word), one
-// 16-byte CAS per probed slot: an empty slot becomes {k, mine}; a slot holding
-// k keeps the smaller tag (older tuples carry tag 0).
-__device__ __forceinline__ void claim(Slot* __restrict__ t, u64 mask, u64 k, u64 mine, u32* flags)
+__device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 mask, u64 k, u64 mine, u64 h, Slot cur,
+                                           u32* flags)
 {
     const Slot empty{kEmpty, ~0ull};
     const Slot mineslot{k, mine};
-    u64 h = mix64(k) & mask;
-    for (u64 probe = 0; probe <= mask; probe++) {
-        Slot cur = atomicCAS(&t[h], empty, mineslot);
-        if (slot_eq(cur, empty)) return;
+    for (u64 probe = 0; probe < kMaxProbe; probe++) {
+        if (slot_eq(cur, empty)) return;   // we inserted it
         if (cur.key == k) {
             while (cur.tag > mine) {
                 const Slot prev = atomicCAS(&t[h], cur, mineslot);
@@ -331,181 +248,390 @@ __device__ __forceinline__ void claim(Slot* __restrict__ t, u64 mask, u64 k, u64
             return;
         }
         h = (h + 1) & mask;
+        cur = atomicCAS(&t[h], empty, mineslot);
     }
     atomicOr(flags, kFlagProbe);
 }
 
-__global__ void __launch_bounds__(kThreads) join_insert_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
-                                                               const u64* __restrict__ off,
-                                                               const u64* __restrict__ start,
-                                                               const u64* __restrict__ inner, Projection pj, int bits,
-                                                               u64* __restrict__ cand, Slot* __restrict__ seen,
-                                                               u64 seen_mask)
+__device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 mask, const u64* key, const u64* mine,
+                                            const bool* valid, u32* flags)
 {
-    __shared__ u64 s_off[kLbsCap];
-    __shared__ u64 s_r0, s_r1;
-    if (ctl->flags) return;
-    const u64 c = ctl->cand_n[rule];
-    if (c == 0) return;
-    const u64 n = rows_n(ctl, outer_ref);
-    const u64* outer = rows_ptr(ctl, outer_ref);
-    const u64 cbase = ctl->cand_base[rule];
-    const u64 tag_base = (ctl->epoch << 40) | cbase;
-    u64* out = cand + cbase;
-    for (u64 p0 = (u64)blockIdx.x * kInsTile; p0 < c; p0 += (u64)gridDim.x * kInsTile) {
-        const u64 p1 = min(c, p0 + kInsTile);
-        if (threadIdx.x == 0) {
-            s_r0 = upper_bound_dev(off, n, p0) - 1;
-            s_r1 = upper_bound_dev(off, n, p1 - 1) - 1;
-        }
-        __syncthreads();
-        const u64 r0 = s_r0, span = s_r1 - s_r0 + 1;
-        const bool staged = span <= (u64)kLbsCap;
-        if (staged)
-            for (u64 i = threadIdx.x; i < span; i += kThreads) s_off[i] = off[r0 + i];
-        __syncthreads();
-        constexpr int kPer = kInsTile / kThreads;
-        u64 okey[kPer], ikey[kPer];
-        u64 pp[kPer];
+    const Slot empty{kEmpty, ~0ull};
+    Slot cur[kClaimBatch];
+    u64 h[kClaimBatch];
 #pragma unroll
-        for (int k = 0; k < kPer; k++) {
-            const u64 p = p0 + threadIdx.x + (u64)k * kThreads;
-            pp[k] = p;
-            okey[k] = ikey[k] = 0;
-            if (p < p1) {
-                const u64 i = staged ? r0 + upper_bound_dev(s_off, span, p) - 1 : upper_bound_dev(off, n, p) - 1;
-                const u64 j = p - (staged ? s_off[i - r0] : off[i]);
-                okey[k] = outer[i];
-                ikey[k] = inner[start[i] + j];
-            }
-        }
+    for (int k = 0; k < kClaimBatch; k++) {
+        h[k] = mix64(key[k]) & mask;
+        if (valid[k]) cur[k] = atomicCAS(&t[h[k]], empty, Slot{key[k], mine[k]});
+    }
 #pragma unroll
-        for (int k = 0; k < kPer; k++) {
-            if (pp[k] >= p1) continue;
-            const u64 key = project(pj, okey[k], ikey[k], bits);
-            out[pp[k]] = key;
-            claim(seen, seen_mask, key, tag_base + pp[k], &ctl->flags);
-        }
-        __syncthreads();
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) copy_insert_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef in_ref,
-                                                               Projection pj,
-                                                               int bits, int pred, u64* __restrict__ cand,
-                                                               Slot* __restrict__ seen, u64 seen_mask)
-{
-    if (ctl->flags) return;
-    const u64 c = ctl->cand_n[rule];
-    if (c == 0) return;
-    const u64* in = rows_ptr(ctl, in_ref);
-    const u64 cbase = ctl->cand_base[rule];
-    const u64 tag_base = (ctl->epoch << 40) | cbase;
-    u64* out = cand + cbase;
-    for (u64 p = (u64)blockIdx.x * kThreads + threadIdx.x; p < c; p += (u64)gridDim.x * kThreads) {
-        const u64 k = in[p];
-        bool keep = true;
-        if (pred != 0) {
-            u64 a = column_of(k, pj.outer_arity, 0, bits);
-            u64 b = pj.outer_arity > 1 ? column_of(k, pj.outer_arity, 1, bits) : 0;
-            keep = eval_pred(pred, a, b);
-        }
-        const u64 key = keep ? project(pj, k, 0, bits) : kEmpty;
-        out[p] = key;
-        if (keep) claim(seen, seen_mask, key, tag_base + p, &ctl->flags);
-    }
+    for (int k = 0; k < kClaimBatch; k++)
+        if (valid[k]) claim_rest(t, mask, key[k], mine[k], h[k], cur[k], flags);
 }
 
 // ---------------------------------------------------------------------------
-// select: winners in candidate order -> staging rows with intern ids
+// join_fused: count + look-back scan + expansion + claim, one launch per rule
 // ---------------------------------------------------------------------------
-constexpr int kSelIpt = 4;
-constexpr int kSelTile = kThreads * kSelIpt;
+constexpr int kJRowsPerThread = 2;
+constexpr int kJRows = kThreads * kJRowsPerThread;   // outer rows per tile
 
-// stage_* are the relation's staging rows (sorted afterwards) or, when
-// `to_log` is set, the relation's log: winners then land directly in its newt
-// region (emission id order, no sort).
-__global__ void __launch_bounds__(kThreads) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, int rule,
-                                                          const u64* __restrict__ cand, const Slot* __restrict__ seen,
-                                                          u64 seen_mask, u64* __restrict__ stage_keys,
-                                                          u64* __restrict__ stage_ids, u64* __restrict__ status,
-                                                          int tile_slot, int passes, int to_log)
+__global__ void __launch_bounds__(kThreads) join_fused_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
+                                                              int outer_shift, const u64* __restrict__ csr,
+                                                              const u64* __restrict__ inner, Projection pj, int bits,
+                                                              u64* __restrict__ cand, u64 cand_cap,
+                                                              Slot* __restrict__ seen, u64 seen_mask,
+                                                              u64* __restrict__ status, int tile_slot)
 {
+    __shared__ u64 s_ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
+    __shared__ u64 s_start[kJRows];    // first inner row of each outer row
+    __shared__ u64 s_key[kJRows];      // outer keys
     __shared__ u64 sm[kWarps + 1];
     __shared__ u32 s_tile;
     __shared__ u64 s_prefix;
-    __shared__ u32 s_hist[kMaxPasses][kRadix];
     if (ctl->flags) return;
-    const u64 c = ctl->cand_n[rule];
-    if (c == 0) return;
-    const int out = plan.rule_out[rule], tslot = plan.rule_tag[rule];
-    // staging offset and intern base: winners of earlier rules into the same relation / tag
-    u64 stage_off = 0, id_ctr = ctl->intern[tslot];
-    for (int q = 0; q < rule; q++) {
-        if (plan.rule_out[q] == out) stage_off += ctl->win_n[q];
-        if (plan.rule_tag[q] == tslot) id_ctr += ctl->win_n[q];
+    const u64 n = rows_n(ctl, outer_ref);
+    const u64* outer = rows_ptr(ctl, outer_ref);
+    if (n == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = 0;
+        return;
     }
-    if (to_log) {
-        const u64 o = ctl->full_n[out] + ctl->delta_n[out];
-        stage_keys += o;
-        stage_ids += o;
-    }
-    const u64 tag_word = plan.rel_tag_word[out];
-    const u64 cbase = ctl->cand_base[rule];
-    const u64 tag_base = (ctl->epoch << 40) | cbase;
-    const u64* in = cand + cbase;
-    const u64 ntiles = (c + kSelTile - 1) / kSelTile;
-    const u32 tag = iter_tag(ctl, tile_slot);
+    const u64 ntiles = (n + kJRows - 1) / kJRows;
     if (blockIdx.x >= ntiles) return;
-    for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kThreads) (&s_hist[0][0])[i] = 0;
+    const u64 cbase = stream_base(ctl, rule);
+    const u64 tag_base = (ctl->epoch << 40) | cbase;
+    const u32 tag = iter_tag(ctl, tile_slot);
+    u32* ctr = tile_counter(ctl, tile_slot);
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->tile_ctr[tile_slot], 1u);
+        if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
         __syncthreads();
         const u64 tile = s_tile;
         __syncthreads();
         if (tile >= ntiles) break;
-        const u64 base = tile * kSelTile + (u64)threadIdx.x * kSelIpt;
-        u64 key[kSelIpt];
-        u32 win = 0;
+        const u64 r0 = tile * kJRows;
+        u64 cnt[kJRowsPerThread];
+        u64 local = 0;
 #pragma unroll
-        for (int k = 0; k < kSelIpt; k++) {
-            const u64 p = base + k;
-            key[k] = kEmpty;
-            if (p < c) {
-                const u64 kk = in[p];
-                if (kk != kEmpty) {
-                    const u64 h = seen_find(seen, seen_mask, kk);
-                    if (h != ~0ull && seen[h].tag == tag_base + p) {
-                        key[k] = kk;
-                        win++;
-                    }
-                }
+        for (int k = 0; k < kJRowsPerThread; k++) {
+            const int li = threadIdx.x * kJRowsPerThread + k;
+            const u64 i = r0 + li;
+            cnt[k] = 0;
+            if (i < n) {
+                const u64 key = outer[i];
+                const u64 j = key >> outer_shift;
+                const u64 s = csr[j];
+                cnt[k] = csr[j + 1] - s;
+                s_start[li] = s;
+                s_key[li] = key;
             }
+            local += cnt[k];
         }
         u64 agg;
-        u64 ex = block_exclusive_scan((u64)win, sm, &agg);
+        u64 ex = block_exclusive_scan(local, sm, &agg);
+#pragma unroll
+        for (int k = 0; k < kJRowsPerThread; k++) {
+            s_ex[threadIdx.x * kJRowsPerThread + k] = ex;
+            ex += cnt[k];
+        }
+        if (threadIdx.x == 0) s_ex[kJRows] = agg;
         if (threadIdx.x < 32) {
             const u64 pre = lookback_warp(status, (u32)tile, agg, tag, &ctl->flags);
             if (threadIdx.x == 0) s_prefix = pre;
         }
         __syncthreads();
-        u64 r = s_prefix + ex;
-#pragma unroll
-        for (int k = 0; k < kSelIpt; k++) {
-            if (key[k] == kEmpty) continue;
-            stage_keys[stage_off + r] = key[k];
-            stage_ids[stage_off + r] = tag_word | (id_ctr + r);
-            for (int ps = 0; ps < passes; ps++)
-                atomicAdd(&s_hist[ps][(key[k] >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
-            r++;
+        const u64 prefix = s_prefix;
+        if (tile == ntiles - 1 && threadIdx.x == 0) {
+            ctl->cand_n[rule] = prefix + agg;
+            ctl->outer_rows += n;
         }
-        if (tile == ntiles - 1 && threadIdx.x == 0) ctl->win_n[rule] = s_prefix + agg;
+        if (cbase + prefix + agg > cand_cap) {
+            if (threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
+        } else {
+            // the tile's candidates: position prefix + j, j in [0, agg)
+            const u64 nr = min((u64)kJRows, n - r0);
+            for (u64 j0 = 0; j0 < agg; j0 += (u64)kThreads * kClaimBatch) {
+                u64 key[kClaimBatch], mine[kClaimBatch];
+                bool valid[kClaimBatch];
+                u64 ik[kClaimBatch];
+                int rr[kClaimBatch];
+                u64 rank[kClaimBatch];
+#pragma unroll
+                for (int k = 0; k < kClaimBatch; k++) {
+                    const u64 j = j0 + threadIdx.x + (u64)k * kThreads;
+                    valid[k] = j < agg;
+                    rr[k] = 0;
+                    rank[k] = 0;
+                    ik[k] = 0;
+                    if (valid[k]) {
+                        rr[k] = (int)upper_bound_dev(s_ex, nr, j) - 1;
+                        rank[k] = j - s_ex[rr[k]];
+                        ik[k] = inner[s_start[rr[k]] + rank[k]];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kClaimBatch; k++) {
+                    const u64 j = j0 + threadIdx.x + (u64)k * kThreads;
+                    key[k] = valid[k] ? project(pj, s_key[rr[k]], ik[k], bits) : 0;
+                    mine[k] = tag_base + prefix + j;
+                    if (valid[k]) cand[cbase + prefix + j] = key[k];
+                }
+                claim_batch(seen, seen_mask, key, mine, valid, &ctl->flags);
+            }
+        }
         __syncthreads();
     }
+}
+
+// copy / copy_filter: one candidate per input row, stream position = row index
+__global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restrict__ ctl, SccPlan plan, int rule,
+                                                              RowsRef in_ref, Projection pj, int bits, int pred,
+                                                              u64* __restrict__ cand, u64 cand_cap,
+                                                              Slot* __restrict__ seen, u64 seen_mask)
+{
+    if (ctl->flags) return;
+    const u64 c = rows_n(ctl, in_ref);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = c;
+    if (c == 0) return;
+    const u64 cbase = stream_base(ctl, rule);
+    if (cbase + c > cand_cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
+        return;
+    }
+    const u64* in = rows_ptr(ctl, in_ref);
+    const u64 tag_base = (ctl->epoch << 40) | cbase;
+    u64* out = cand + cbase;
+    const u64 stride = (u64)gridDim.x * kThreads * kClaimBatch;
+    for (u64 p0 = (u64)blockIdx.x * kThreads * kClaimBatch; p0 < c; p0 += stride) {
+        u64 key[kClaimBatch], mine[kClaimBatch];
+        bool valid[kClaimBatch];
+#pragma unroll
+        for (int k = 0; k < kClaimBatch; k++) {
+            const u64 p = p0 + threadIdx.x + (u64)k * kThreads;
+            valid[k] = false;
+            key[k] = 0;
+            mine[k] = tag_base + p;
+            if (p < c) {
+                const u64 kk = in[p];
+                bool keep = true;
+                if (pred != 0) {
+                    u64 a = column_of(kk, pj.outer_arity, 0, bits);
+                    u64 b = pj.outer_arity > 1 ? column_of(kk, pj.outer_arity, 1, bits) : 0;
+                    keep = eval_pred(pred, a, b);
+                }
+                key[k] = keep ? project(pj, kk, 0, bits) : kEmpty;
+                out[p] = key[k];
+                valid[k] = keep;
+            }
+        }
+        claim_batch(seen, seen_mask, key, mine, valid, &ctl->flags);
+    }
+    (void)plan;
+}
+
+// ---------------------------------------------------------------------------
+// end of an iteration (one thread): semi-naive swap on the counters, history,
+// intern counters, next bank of tile counters, graph condition.
+// ---------------------------------------------------------------------------
+struct SccRelMap {
+    int n_rules_in[kMaxSccRels];
+    int rules_in[kMaxSccRels][kMaxSccRules];
+};
+
+__device__ void end_of_iteration(IterCtl* __restrict__ ctl, const SccPlan& plan, const SccRelMap& rm,
+                                 u64* __restrict__ history, cudaGraphConditionalHandle cond, int use_cond)
+{
+    bool cont = false;
+    const bool records = !plan.fixpoint || ctl->batch_pos + 1 >= plan.batch_size;
+    if (ctl->flags == 0 && records && ctl->hist_n >= plan.hist_cap) atomicOr(&ctl->flags, kFlagOverflow);
+    if (ctl->flags == 0) {
+        u64 sum_delta = 0, sum_full = 0, added = 0;
+        bool grow = false;
+        for (int s = 0; s < plan.n_rels; s++) {
+            u64 nn = 0, in = 0;
+            for (int q = 0; q < rm.n_rules_in[s]; q++) {
+                nn += ctl->win_n[rm.rules_in[s][q]];
+                in += ctl->cand_n[rm.rules_in[s][q]];
+            }
+            // relation::insert_delta_in_full + local_insert_in_delta
+            if (ctl->delta_n[s]) ctl->runs[s]++;
+            ctl->full_n[s] += ctl->delta_n[s];
+            ctl->delta_n[s] = nn;
+            ctl->seen_n[s] += nn;
+            added += nn;
+            sum_delta += ctl->delta_n[s];
+            sum_full += ctl->full_n[s];
+            if (rm.n_rules_in[s] && ctl->seen_n[s] + 2 * in > plan.seen_limit[s]) grow = true;
+        }
+        u64 tag_add[kMaxTagSlots] = {0};
+        for (int r = 0; r < plan.n_rules; r++) tag_add[plan.rule_tag[r]] += ctl->win_n[r];
+        for (int t = 0; t < kMaxTagSlots; t++) ctl->intern[t] += tag_add[t];
+        u64 cands = 0;
+        for (int r = 0; r < plan.n_rules; r++) cands += ctl->cand_n[r];
+        ctl->candidates += cands;
+        ctl->new_tuples += added;
+        ctl->iteration++;
+        ctl->epoch++;
+        ctl->batch_pos++;
+        cont = true;
+        if (records) {
+            ctl->batch_pos = 0;
+            history[2 * ctl->hist_n] = sum_delta;
+            history[2 * ctl->hist_n + 1] = sum_full;
+            ctl->hist_n++;
+            cont = plan.fixpoint && sum_delta != 0;
+        }
+        if (ctl->iteration >= plan.iter_limit) cont = false;
+        ctl->done = cont ? 0u : 1u;
+        if (cont && grow) {
+            atomicOr(&ctl->flags, kFlagGrow);
+            cont = false;
+        }
+        // the next iteration's bank of tile counters (used last by the previous iteration)
+        for (int i = 0; i < kTileSlots; i++) ctl->tile_ctr[(ctl->iteration & 1) * kTileSlots + i] = 0;
+    }
+    if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------
+// select: winners in candidate order -> the relation's log (emission ids) or
+// its staging rows (reference ids, sorted afterwards)
+// ---------------------------------------------------------------------------
+constexpr int kSelIpt = 4;
+constexpr int kSelTile = kThreads * kSelIpt;
+
+struct SelectArgs {
+    int rule;
+    int last;                 // last rule of the iteration: runs the iteration end
+    u64* dst_keys;            // log (to_log) or staging rows
+    u64* dst_ids;
+    int to_log;
+    int passes;               // digit histograms to accumulate (reference ids)
+    u64 log_cap;              // rows the output relation's log holds
+    u64 stage_cap;
+};
+
+__global__ void __launch_bounds__(kThreads) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
+                                                          SelectArgs a, const u64* __restrict__ cand,
+                                                          const Slot* __restrict__ seen, u64 seen_mask,
+                                                          u64* __restrict__ status, int tile_slot,
+                                                          u64* __restrict__ history, cudaGraphConditionalHandle cond,
+                                                          int use_cond)
+{
+    __shared__ u64 sm[kWarps + 1];
+    __shared__ u32 s_tile;
+    __shared__ u64 s_prefix;
+    __shared__ u32 s_hist[kMaxPasses][kRadix];
+    const int rule = a.rule;
+    const u64 c = ctl->cand_n[rule];
+    const int out = plan.rule_out[rule], tslot = plan.rule_tag[rule];
+    bool active = ctl->flags == 0;
+    if (active) {
+        // room for every candidate of every rule into this relation, checked before any write
+        u64 incoming = 0;
+        for (int q = 0; q < rm.n_rules_in[out]; q++) incoming += ctl->cand_n[rm.rules_in[out][q]];
+        // the new delta lands in the log either way (directly, or via staging + sort)
+        const bool over = ctl->full_n[out] + ctl->delta_n[out] + incoming > a.log_cap ||
+                          (!a.to_log && incoming > a.stage_cap);
+        if (over) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
+            active = false;
+        }
+    }
+    if (c == 0 && blockIdx.x == 0 && threadIdx.x == 0) ctl->win_n[rule] = 0;
+    const u64 ntiles = (c + kSelTile - 1) / kSelTile;
+    if (active && c > 0 && blockIdx.x < ntiles) {
+        // destination offset and intern base: winners of earlier rules into the same relation / tag
+        u64 dst_off = 0, id_ctr = ctl->intern[tslot];
+        for (int q = 0; q < rule; q++) {
+            if (plan.rule_out[q] == out) dst_off += ctl->win_n[q];
+            if (plan.rule_tag[q] == tslot) id_ctr += ctl->win_n[q];
+        }
+        u64* dk = a.dst_keys;
+        u64* dv = a.dst_ids;
+        if (a.to_log) dst_off += ctl->full_n[out] + ctl->delta_n[out];
+        const u64 tag_word = plan.rel_tag_word[out];
+        const u64 cbase = stream_base(ctl, rule);
+        const u64 tag_base = (ctl->epoch << 40) | cbase;
+        const u64* in = cand + cbase;
+        const u32 tag = iter_tag(ctl, tile_slot);
+        u32* ctr = tile_counter(ctl, tile_slot);
+        for (int i = threadIdx.x; i < a.passes * kRadix; i += kThreads) (&s_hist[0][0])[i] = 0;
+        for (;;) {
+            if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+            __syncthreads();
+            const u64 tile = s_tile;
+            __syncthreads();
+            if (tile >= ntiles) break;
+            const u64 base = tile * kSelTile + (u64)threadIdx.x * kSelIpt;
+            u64 key[kSelIpt];
+            u64 h[kSelIpt];
+            Slot cur[kSelIpt];
+#pragma unroll
+            for (int k = 0; k < kSelIpt; k++) {
+                const u64 p = base + k;
+                key[k] = p < c ? in[p] : kEmpty;
+            }
+#pragma unroll
+            for (int k = 0; k < kSelIpt; k++) {
+                h[k] = mix64(key[k]) & seen_mask;
+                cur[k] = Slot{kEmpty, 0};
+                if (key[k] != kEmpty) {
+                    const ulonglong2 w = __ldcg((const ulonglong2*)&seen[h[k]]);
+                    cur[k] = Slot{w.x, w.y};
+                }
+            }
+            u32 win = 0;
+#pragma unroll
+            for (int k = 0; k < kSelIpt; k++) {
+                if (key[k] == kEmpty) continue;
+                u64 hh = h[k];
+                Slot sl = cur[k];
+                u64 probe = 0;
+                while (sl.key != key[k] && sl.key != kEmpty && probe < kMaxProbe) {
+                    hh = (hh + 1) & seen_mask;
+                    sl = seen[hh];
+                    probe++;
+                }
+                if (sl.key == key[k] && sl.tag == tag_base + base + k) win++;
+                else key[k] = kEmpty;
+            }
+            u64 agg;
+            u64 ex = block_exclusive_scan((u64)win, sm, &agg);
+            if (threadIdx.x < 32) {
+                const u64 pre = lookback_warp(status, (u32)tile, agg, tag, &ctl->flags);
+                if (threadIdx.x == 0) s_prefix = pre;
+            }
+            __syncthreads();
+            u64 r = s_prefix + ex;
+#pragma unroll
+            for (int k = 0; k < kSelIpt; k++) {
+                if (key[k] == kEmpty) continue;
+                dk[dst_off + r] = key[k];
+                dv[dst_off + r] = tag_word | (id_ctr + r);
+                for (int ps = 0; ps < a.passes; ps++)
+                    atomicAdd(&s_hist[ps][(key[k] >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
+                r++;
+            }
+            if (tile == ntiles - 1 && threadIdx.x == 0) ctl->win_n[rule] = s_prefix + agg;
+            __syncthreads();
+        }
+        if (a.passes) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < a.passes * kRadix; i += kThreads) {
+                const u32 v = (&s_hist[0][0])[i];
+                if (v) atomicAdd(&ctl->sort_hist[out][i / kRadix][i % kRadix], (u64)v);
+            }
+        }
+    }
+    // the last block to finish runs the iteration end (after every write of this launch)
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
-        const u32 v = (&s_hist[0][0])[i];
-        if (v) atomicAdd(&ctl->sort_hist[out][i / kRadix][i % kRadix], (u64)v);
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const u32 done = atomicAdd(&ctl->exit_ctr, 1u);
+        if (done == gridDim.x - 1) {
+            __threadfence();
+            ctl->exit_ctr = 0;
+            if (a.last) end_of_iteration(ctl, plan, rm, history, cond, use_cond);
+        }
     }
 }
 
@@ -523,6 +649,7 @@ struct SortPassArgs {
     u64* dst_k;               // when dst_log: the log base (rows go to base + full_n + delta_n)
     u64* dst_v;
     int dst_log;
+    u64 log_cap;              // rows the relation's log holds (dst_log)
     int n_rules_in;           // rules writing this relation
     int rules_in[kMaxSccRules];
 };
@@ -548,6 +675,10 @@ __global__ void __launch_bounds__(kThreads) sort_pass_kernel(IterCtl* __restrict
     u64* dv = a.dst_v;
     if (a.dst_log) {
         const u64 o = ctl->full_n[a.rel] + ctl->delta_n[a.rel];
+        if (o + n > a.log_cap) {   // select checks this first; never write past the log
+            if (threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
+            return;
+        }
         dk += o;
         dv += o;
     }
@@ -558,7 +689,7 @@ __global__ void __launch_bounds__(kThreads) sort_pass_kernel(IterCtl* __restrict
         s_gstart[threadIdx.x] = block_exclusive_scan(ctl->sort_hist[a.rel][a.pass][threadIdx.x], sm, &tot);
     }
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->tile_ctr[tile_slot], 1u);
+        if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter(ctl, tile_slot), 1u);
         for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&s_wcnt[0][0])[i] = 0;
         __syncthreads();
         const u64 tile = s_tile;
@@ -646,67 +777,15 @@ __global__ void __launch_bounds__(kThreads) sort_pass_kernel(IterCtl* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// iter_end: semi-naive swap on the counters, history, graph condition
+// iteration end as its own launch (reference id order: after the sort passes)
 // ---------------------------------------------------------------------------
-struct SccRelMap {
-    int n_rules_in[kMaxSccRels];
-    int rules_in[kMaxSccRels][kMaxSccRules];
-};
-
 __global__ void iter_end_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm, u64* __restrict__ history,
                                 cudaGraphConditionalHandle cond, int use_cond)
 {
-    // every block clears this iteration's sort histograms
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < (u64)kMaxSccRels * kMaxPasses * kRadix;
          i += (u64)gridDim.x * blockDim.x)
         (&ctl->sort_hist[0][0][0])[i] = 0;
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    bool cont = false;
-    if (ctl->flags == 0) {
-        u64 sum_delta = 0, sum_full = 0, added = 0;
-        for (int s = 0; s < plan.n_rels; s++) {
-            u64 nn = 0;
-            for (int q = 0; q < rm.n_rules_in[s]; q++) nn += ctl->win_n[rm.rules_in[s][q]];
-            // relation::insert_delta_in_full + local_insert_in_delta
-            if (ctl->delta_n[s]) ctl->runs[s]++;
-            ctl->full_n[s] += ctl->delta_n[s];
-            ctl->delta_n[s] = nn;
-            ctl->seen_n[s] += nn;
-            added += nn;
-            sum_delta += ctl->delta_n[s];
-            sum_full += ctl->full_n[s];
-        }
-        u64 tag_add[kMaxTagSlots] = {0};
-        for (int r = 0; r < plan.n_rules; r++) tag_add[plan.rule_tag[r]] += ctl->win_n[r];
-        for (int t = 0; t < kMaxTagSlots; t++) ctl->intern[t] += tag_add[t];
-        ctl->new_tuples += added;
-        ctl->iteration++;
-        ctl->epoch++;
-        ctl->batch_pos++;
-        cont = true;
-        if (!plan.fixpoint) {
-            // non-fixpoint SCC: one iteration, one history entry
-            history[2 * ctl->hist_n] = sum_delta;
-            history[2 * ctl->hist_n + 1] = sum_full;
-            ctl->hist_n++;
-            cont = false;
-        } else if (ctl->batch_pos >= plan.batch_size) {
-            ctl->batch_pos = 0;
-            if (ctl->hist_n >= plan.hist_cap) {
-                atomicOr(&ctl->flags, kFlagHistory);
-                cont = false;
-            } else {
-                history[2 * ctl->hist_n] = sum_delta;
-                history[2 * ctl->hist_n + 1] = sum_full;
-                ctl->hist_n++;
-                cont = sum_delta != 0;
-            }
-        }
-        if (ctl->iteration >= plan.iter_limit) cont = false;
-        ctl->done = cont ? 0u : 1u;
-    }
-    for (int i = 0; i < kTileSlots; i++) ctl->tile_ctr[i] = 0;
-    if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+    if (blockIdx.x == 0 && threadIdx.x == 0) end_of_iteration(ctl, plan, rm, history, cond, use_cond);
 }
 
 }  // namespace ra

@@ -22,7 +22,7 @@ IDS_EMISSION, IDS_REFERENCE = 0, 1
 # every entry point declared in include/ra_engine.h
 EXPORTS = (
     "ra_program_create", "ra_program_destroy", "ra_program_set_stream", "ra_program_set_batch_size",
-    "ra_program_set_id_order",
+    "ra_program_set_id_order", "ra_program_set_launch_timing",
     "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
     "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats",
@@ -65,6 +65,7 @@ def lib():
         L.ra_program_set_stream.argtypes = [P, P]
         L.ra_program_set_batch_size.argtypes = [P, C.c_uint32]
         L.ra_program_set_id_order.argtypes = [P, C.c_int]
+        L.ra_program_set_launch_timing.argtypes = [P, C.c_int]
         L.ra_relation_create.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int, i32p]
         L.ra_relation_load_rows.argtypes = [P, C.c_int, u64p, C.c_uint64]
         L.ra_relation_load_rows_device.argtypes = [P, C.c_int, C.c_void_p, C.c_uint64]
@@ -130,6 +131,10 @@ class Program:
     def set_id_order(self, mode: int):
         """IDS_EMISSION (default) or IDS_REFERENCE (single-rank reference numbering)."""
         self._ck(self._L.ra_program_set_id_order(self._p, mode), "set_id_order")
+
+    def set_launch_timing(self, on: bool):
+        """Per-launch CUDA events on every iteration kernel (no CUDA graph while on)."""
+        self._ck(self._L.ra_program_set_launch_timing(self._p, int(bool(on))), "set_launch_timing")
 
     def set_batch_size(self, n: int):
         self._ck(self._L.ra_program_set_batch_size(self._p, n), "set_batch_size")
