@@ -48,7 +48,7 @@ WORKLOADS = {
 # bounded CPU sample of the same graph family (mean out-degree 0.95)
 CPU_SAMPLE = (1 << 17, round(0.95 * (1 << 17)), 2)
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) per launch of join_insert_kernel from the ncu capture
+# DRAM bytes (read + write) per launch of join_fused_kernel from the ncu capture
 # summarised in profiles/ (None until captured for this kernel version)
 TRAFFIC_PER_LAUNCH = None
 
@@ -221,7 +221,7 @@ def run_ours(args, rank, world, local_rank):
     value = tc_all * args.steps / (total_ms / 1e3)
     st = prog.stats()
 
-    # dominant kernel (fused join expansion + first-occurrence claim): per-launch
+    # dominant kernel (fused join count, scan, expansion + first-occurrence claim): per-launch
     # CUDA events on the engine's stream, in an instrumented pass over the same
     # program (the timed steps run as one CUDA graph, whose nodes events cannot split)
     prog.set_launch_timing(True)
@@ -266,7 +266,7 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = load_peaks()
     achieved = (dedup_bytes / dedup_launches) / ((dedup_ms / dedup_launches) / 1e3) / 1e9 if dedup_launches else 0.0
-    roofline = {"kernel": "join_insert_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roofline = {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": TRAFFIC_PER_LAUNCH,
                 "launches": int(dedup_launches), "avg_launch_us": 1e3 * dedup_ms / max(dedup_launches, 1),
                 "bytes_per_launch": dedup_bytes / max(dedup_launches, 1),
