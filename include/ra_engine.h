@@ -170,6 +170,26 @@ int ra_relation_counts(ra_program* p, int rel, uint64_t* full, uint64_t* delta);
 int ra_relation_dump_full(ra_program* p, int rel, uint64_t* host_rows, uint64_t cap_rows,
                           uint64_t* rows_out);
 
+/* Largest row count ra_rows_distinct_noalloc accepts. */
+#define RA_NOALLOC_MAX_ROWS (1u << 17)
+
+/* No counterpart in the reference.  Sorts nrows rows of arity+1 u64 (data
+ * columns, then the id column) lexicographically and drops exact duplicates --
+ * the full version a relation holds after loading those rows -- without
+ * allocating device memory, for callers that cannot call cudaMalloc (a runtime
+ * that reserved the whole GPU up front, a latency-critical thread that must not
+ * take cudaMalloc's implicit synchronisation, a host that forbids the CUDA
+ * allocator).  dev_rows, dev_out_rows (room for nrows rows) and dev_out_nrows
+ * are device pointers; stream is a cudaStream_t (0 = legacy default stream).
+ * Returns RA_E_BADARG when nrows > RA_NOALLOC_MAX_ROWS.
+ * Scratch is one fixed static device array (about 6 MB, held on every GPU
+ * that loads the library until exit).  The first call on a device looks up
+ * that array's device address, so make it before any stream capture on that
+ * device.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+int ra_rows_distinct_noalloc(const uint64_t* dev_rows, uint64_t nrows, uint32_t arity,
+                             uint64_t* dev_out_rows, uint64_t* dev_out_nrows, void* stream);
+
 const char* ra_status_string(int status);
 /* Message of the last failing call on this program ("" if none). */
 const char* ra_last_error(ra_program* p);

@@ -1861,3 +1861,7 @@ const char* ra_status_string(int status)
 const char* ra_last_error(ra_program* p) { return p ? p->err.c_str() : "null program"; }
 
 }  // extern "C"
+
+// The scratch-free load-path entry point shares this translation unit (and its
+// header-defined kernels); its static scratch array is defined in that file.
+#include "ra_noalloc.cu"

@@ -26,7 +26,7 @@ EXPORTS = (
     "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
     "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats",
-    "ra_relation_counts", "ra_relation_dump_full", "ra_status_string", "ra_last_error",
+    "ra_relation_counts", "ra_relation_dump_full", "ra_rows_distinct_noalloc", "ra_status_string", "ra_last_error",
 )
 
 
@@ -82,6 +82,7 @@ def lib():
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
         L.ra_relation_counts.argtypes = [P, C.c_int, u64p, u64p]
         L.ra_relation_dump_full.argtypes = [P, C.c_int, u64p, C.c_uint64, u64p]
+        L.ra_rows_distinct_noalloc.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ra_status_string.argtypes = [C.c_int]
         L.ra_status_string.restype = C.c_char_p
         L.ra_last_error.argtypes = [P]
