@@ -48,9 +48,11 @@ WORKLOADS = {
 # bounded CPU sample of the same graph family (mean out-degree 0.95)
 CPU_SAMPLE = (1 << 17, round(0.95 * (1 << 17)), 2)
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) per launch of join_fused_kernel from the ncu capture
-# summarised in profiles/ (None until captured for this kernel version)
-TRAFFIC_PER_LAUNCH = None
+# DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
+# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.75 / 1.81 / 1.76 over
+# three launches of the same graph family at 1/4 scale); bench's `traffic` is
+# this ratio times the algorithmic bytes of an average tc-er22 launch.
+TRAFFIC_PER_ALGO_BYTE = 1.77
 
 
 def load_peaks():
@@ -267,7 +269,9 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = load_peaks()
     achieved = (dedup_bytes / dedup_launches) / ((dedup_ms / dedup_launches) / 1e3) / 1e9 if dedup_launches else 0.0
     roofline = {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": TRAFFIC_PER_LAUNCH,
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": TRAFFIC_PER_ALGO_BYTE * dedup_bytes / max(dedup_launches, 1),
+                "traffic_note": "ncu DRAM read+write per launch, measured on tc-er20 and scaled by units processed",
                 "launches": int(dedup_launches), "avg_launch_us": 1e3 * dedup_ms / max(dedup_launches, 1),
                 "bytes_per_launch": dedup_bytes / max(dedup_launches, 1),
                 "bytes_model": "48 B per candidate (8 B inner key read, 8 B candidate write, 16 B seen-slot read "
