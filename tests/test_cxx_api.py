@@ -110,3 +110,18 @@ def test_cxx_api_matches_goldens(tmp_path, name, id_order):
             assert rows_digest(got) == exp["sha256"], rname
         else:
             assert rows_digest(np.ascontiguousarray(got[:, :-1])) == exp["data_sha256"], rname
+
+
+@pytest.mark.gpu
+def test_integration_ctypes_snippet_runs(tmp_path):
+    """The ctypes example in INTEGRATION.md computes TC of a 2-edge chain (3 pairs)."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = text.split("```python", 1)[1].split("```", 1)[0]
+    env = {}
+    cwd = os.getcwd()
+    os.chdir(ROOT)
+    try:
+        exec(compile(block, "INTEGRATION.md", "exec"), env)
+    finally:
+        os.chdir(cwd)
+    assert env["f"].value == 3
