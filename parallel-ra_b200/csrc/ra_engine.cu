@@ -162,6 +162,7 @@ struct ra_program {
     IterCtl* ctl = nullptr;
     IterCtl* hctl = nullptr;      // pinned mirror (header part)
     u64* dcand = nullptr;
+    u32* dloser = nullptr;        // per stream position: epoch in which it lost (not a first occurrence)
     u64 dcand_cap = 0;
     u64* doff[kMaxSccRules] = {};
     u64* dstart[kMaxSccRules] = {};
@@ -943,7 +944,10 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
 {
     if (cand_cap > p->dcand_cap) {
         dev_free(p, &p->dcand);
+        dev_free(p, &p->dloser);
         dev_alloc(p, &p->dcand, cand_cap);
+        dev_alloc(p, &p->dloser, cand_cap);
+        CK(cudaMemsetAsync(p->dloser, 0, cand_cap * 4, p->stream));   // epoch 0: no marks
         p->dcand_cap = cand_cap;
     }
     const bool ref = p->id_order == RA_IDS_REFERENCE;
@@ -1029,10 +1033,11 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         if (r.kind == kJoin)
             join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
                                                              p->bits, p->dcand, p->dcand_cap, out.seen,
-                                                             out.seen_cap - 1, p->status, slot++);
+                                                             out.seen_cap - 1, p->dloser, p->status, slot++);
         else
             copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
-                                                                 p->dcand, p->dcand_cap, out.seen, out.seen_cap - 1);
+                                                                 p->dcand, p->dcand_cap, out.seen, out.seen_cap - 1,
+                                                                 p->dloser);
         launches++;
     }
     for (int q = 0; q < pl.n_rules; q++) {
@@ -1048,8 +1053,8 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         a.passes = ref ? d.passes[r.out_slot] : 0;
         a.log_cap = out.cap;
         a.stage_cap = p->stage_cap;
-        select_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, out.seen, out.seen_cap - 1,
-                                                     p->status, slot++, p->dhist, cond, use_cond);
+        select_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, p->dloser, p->status, slot++,
+                                                     p->dhist, cond, use_cond);
         launches++;
     }
     if (ref) {
@@ -1102,8 +1107,8 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
         put(&r.seen_cap, sizeof r.seen_cap);
         put(&r.cap, sizeof r.cap);
     }
-    const void* scratch[8] = {p->ctl, p->dcand, p->status, p->dhist, p->sort_k[0], p->sort_k[1], p->sort_v[0],
-                              p->sort_v[1]};
+    const void* scratch[9] = {p->ctl, p->dcand, p->status, p->dhist, p->sort_k[0], p->sort_k[1], p->sort_v[0],
+                              p->sort_v[1], p->dloser};
     put(scratch, sizeof scratch);
     put(p->stage_k, sizeof p->stage_k);
     put(p->stage_v, sizeof p->stage_v);
@@ -1386,7 +1391,7 @@ void reset_state(ra_program* p)
     p->intern.clear();
     p->executed = false;
     p->running = false;
-    p->epoch = 0;
+    // p->epoch keeps counting across runs: loser marks and seen-set tags are epoch-stamped
 }
 
 void begin_run(ra_program* p)
@@ -1565,6 +1570,7 @@ int ra_program_destroy(ra_program* p)
     dev_free(p, &p->hist_off);
     dev_free(p, &p->ctl);
     dev_free(p, &p->dcand);
+    dev_free(p, &p->dloser);
     for (int q = 0; q < kMaxSccRules; q++) {
         dev_free(p, &p->doff[q]);
         dev_free(p, &p->dstart[q]);

@@ -228,24 +228,43 @@ __device__ __forceinline__ u64 stream_base(const IterCtl* c, int rule)
 // ---------------------------------------------------------------------------
 // first-occurrence claims: one 16-byte CAS per probed slot.  An empty slot
 // becomes {k, mine}; a slot holding k keeps the smaller tag (older tuples carry
-// tag 0).  kClaimBatch independent claims are issued back to back.
+// smaller tags: 0, or an earlier epoch).  Every candidate that is not the first
+// occurrence of a new tuple ends up marked in `loser` (indexed by stream
+// position, value = epoch): it marks itself when the key is older or holds a
+// smaller position, and marks the position it displaces when it lowers the
+// tag.  select then needs no access to the seen set.  kClaimBatch independent
+// claims are issued back to back.
 // ---------------------------------------------------------------------------
 constexpr int kClaimBatch = 4;
+constexpr u64 kPosMask = (1ull << 40) - 1;
+
+struct LoserMarks {
+    u32* mark;      // per stream position
+    u32 epoch;      // marks of this iteration (older values mean "not a loser now")
+    u64 epoch_tag;  // epoch << 40: tags below it belong to tuples from earlier iterations
+};
 
 __device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 mask, u64 k, u64 mine, u64 h, Slot cur,
-                                           u32* flags)
+                                           const LoserMarks& lm, u32* flags)
 {
     const Slot empty{kEmpty, ~0ull};
     const Slot mineslot{k, mine};
     for (u64 probe = 0; probe < kMaxProbe; probe++) {
         if (slot_eq(cur, empty)) return;   // we inserted it
         if (cur.key == k) {
-            while (cur.tag > mine) {
+            for (;;) {
+                if (cur.tag == mine) return;     // our own claim from an attempt being replayed
+                if (cur.tag < mine) {            // older tuple, or an earlier position this iteration
+                    lm.mark[mine & kPosMask] = lm.epoch;
+                    return;
+                }
                 const Slot prev = atomicCAS(&t[h], cur, mineslot);
-                if (slot_eq(prev, cur)) return;
+                if (slot_eq(prev, cur)) {      // we took the slot from a later position
+                    lm.mark[cur.tag & kPosMask] = lm.epoch;
+                    return;
+                }
                 cur = prev;
             }
-            return;
         }
         h = (h + 1) & mask;
         cur = atomicCAS(&t[h], empty, mineslot);
@@ -254,7 +273,7 @@ __device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 mask, u64 k
 }
 
 __device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 mask, const u64* key, const u64* mine,
-                                            const bool* valid, u32* flags)
+                                            const bool* valid, const LoserMarks& lm, u32* flags)
 {
     const Slot empty{kEmpty, ~0ull};
     Slot cur[kClaimBatch];
@@ -266,21 +285,39 @@ __device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 mask, cons
     }
 #pragma unroll
     for (int k = 0; k < kClaimBatch; k++)
-        if (valid[k]) claim_rest(t, mask, key[k], mine[k], h[k], cur[k], flags);
+        if (valid[k]) claim_rest(t, mask, key[k], mine[k], h[k], cur[k], lm, flags);
+}
+
+__device__ __forceinline__ LoserMarks loser_marks(const IterCtl* c, u32* mark)
+{
+    return LoserMarks{mark, (u32)c->epoch, c->epoch << 40};
 }
 
 // ---------------------------------------------------------------------------
 // join_fused: count + look-back scan + expansion + claim, one launch per rule
 // ---------------------------------------------------------------------------
-constexpr int kJRowsPerThread = 2;
+#ifndef RA_JOIN_ROWS_PER_THREAD
+#define RA_JOIN_ROWS_PER_THREAD 2
+#endif
+#ifndef RA_JOIN_MIN_BLOCKS
+#define RA_JOIN_MIN_BLOCKS 4
+#endif
+#ifndef RA_SELECT_IPT
+#define RA_SELECT_IPT 4
+#endif
+#ifndef RA_SELECT_MIN_BLOCKS
+#define RA_SELECT_MIN_BLOCKS 4
+#endif
+constexpr int kJRowsPerThread = RA_JOIN_ROWS_PER_THREAD;
 constexpr int kJRows = kThreads * kJRowsPerThread;   // outer rows per tile
 
-__global__ void __launch_bounds__(kThreads) join_fused_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
+__global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
                                                               int outer_shift, const u64* __restrict__ csr,
                                                               const u64* __restrict__ inner, Projection pj, int bits,
                                                               u64* __restrict__ cand, u64 cand_cap,
                                                               Slot* __restrict__ seen, u64 seen_mask,
-                                                              u64* __restrict__ status, int tile_slot)
+                                                              u32* __restrict__ loser, u64* __restrict__ status,
+                                                              int tile_slot)
 {
     __shared__ u64 s_ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
     __shared__ u64 s_start[kJRows];    // first inner row of each outer row
@@ -301,6 +338,7 @@ __global__ void __launch_bounds__(kThreads) join_fused_kernel(IterCtl* __restric
     const u64 tag_base = (ctl->epoch << 40) | cbase;
     const u32 tag = iter_tag(ctl, tile_slot);
     u32* ctr = tile_counter(ctl, tile_slot);
+    const LoserMarks lm = loser_marks(ctl, loser);
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
         __syncthreads();
@@ -374,7 +412,7 @@ __global__ void __launch_bounds__(kThreads) join_fused_kernel(IterCtl* __restric
                     mine[k] = tag_base + prefix + j;
                     if (valid[k]) cand[cbase + prefix + j] = key[k];
                 }
-                claim_batch(seen, seen_mask, key, mine, valid, &ctl->flags);
+                claim_batch(seen, seen_mask, key, mine, valid, lm, &ctl->flags);
             }
         }
         __syncthreads();
@@ -385,7 +423,8 @@ __global__ void __launch_bounds__(kThreads) join_fused_kernel(IterCtl* __restric
 __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restrict__ ctl, SccPlan plan, int rule,
                                                               RowsRef in_ref, Projection pj, int bits, int pred,
                                                               u64* __restrict__ cand, u64 cand_cap,
-                                                              Slot* __restrict__ seen, u64 seen_mask)
+                                                              Slot* __restrict__ seen, u64 seen_mask,
+                                                              u32* __restrict__ loser)
 {
     if (ctl->flags) return;
     const u64 c = rows_n(ctl, in_ref);
@@ -398,6 +437,7 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
     }
     const u64* in = rows_ptr(ctl, in_ref);
     const u64 tag_base = (ctl->epoch << 40) | cbase;
+    const LoserMarks lm = loser_marks(ctl, loser);
     u64* out = cand + cbase;
     const u64 stride = (u64)gridDim.x * kThreads * kClaimBatch;
     for (u64 p0 = (u64)blockIdx.x * kThreads * kClaimBatch; p0 < c; p0 += stride) {
@@ -422,7 +462,7 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
                 valid[k] = keep;
             }
         }
-        claim_batch(seen, seen_mask, key, mine, valid, &ctl->flags);
+        claim_batch(seen, seen_mask, key, mine, valid, lm, &ctl->flags);
     }
     (void)plan;
 }
@@ -495,7 +535,7 @@ __device__ void end_of_iteration(IterCtl* __restrict__ ctl, const SccPlan& plan,
 // select: winners in candidate order -> the relation's log (emission ids) or
 // its staging rows (reference ids, sorted afterwards)
 // ---------------------------------------------------------------------------
-constexpr int kSelIpt = 4;
+constexpr int kSelIpt = RA_SELECT_IPT;
 constexpr int kSelTile = kThreads * kSelIpt;
 
 struct SelectArgs {
@@ -509,9 +549,9 @@ struct SelectArgs {
     u64 stage_cap;
 };
 
-__global__ void __launch_bounds__(kThreads) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
+__global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
                                                           SelectArgs a, const u64* __restrict__ cand,
-                                                          const Slot* __restrict__ seen, u64 seen_mask,
+                                                          const u32* __restrict__ loser,
                                                           u64* __restrict__ status, int tile_slot,
                                                           u64* __restrict__ history, cudaGraphConditionalHandle cond,
                                                           int use_cond)
@@ -550,7 +590,7 @@ __global__ void __launch_bounds__(kThreads) select_kernel(IterCtl* __restrict__ 
         if (a.to_log) dst_off += ctl->full_n[out] + ctl->delta_n[out];
         const u64 tag_word = plan.rel_tag_word[out];
         const u64 cbase = stream_base(ctl, rule);
-        const u64 tag_base = (ctl->epoch << 40) | cbase;
+        const u32 ep = (u32)ctl->epoch;
         const u64* in = cand + cbase;
         const u32 tag = iter_tag(ctl, tile_slot);
         u32* ctr = tile_counter(ctl, tile_slot);
@@ -563,36 +603,18 @@ __global__ void __launch_bounds__(kThreads) select_kernel(IterCtl* __restrict__ 
             if (tile >= ntiles) break;
             const u64 base = tile * kSelTile + (u64)threadIdx.x * kSelIpt;
             u64 key[kSelIpt];
-            u64 h[kSelIpt];
-            Slot cur[kSelIpt];
-#pragma unroll
-            for (int k = 0; k < kSelIpt; k++) {
-                const u64 p = base + k;
-                key[k] = p < c ? in[p] : kEmpty;
-            }
-#pragma unroll
-            for (int k = 0; k < kSelIpt; k++) {
-                h[k] = mix64(key[k]) & seen_mask;
-                cur[k] = Slot{kEmpty, 0};
-                if (key[k] != kEmpty) {
-                    const ulonglong2 w = __ldcg((const ulonglong2*)&seen[h[k]]);
-                    cur[k] = Slot{w.x, w.y};
-                }
-            }
             u32 win = 0;
 #pragma unroll
             for (int k = 0; k < kSelIpt; k++) {
-                if (key[k] == kEmpty) continue;
-                u64 hh = h[k];
-                Slot sl = cur[k];
-                u64 probe = 0;
-                while (sl.key != key[k] && sl.key != kEmpty && probe < kMaxProbe) {
-                    hh = (hh + 1) & seen_mask;
-                    sl = seen[hh];
-                    probe++;
+                const u64 p = base + k;
+                key[k] = kEmpty;
+                if (p < c) {
+                    const u64 kk = in[p];
+                    if (kk != kEmpty && loser[cbase + p] != ep) {
+                        key[k] = kk;
+                        win++;
+                    }
                 }
-                if (sl.key == key[k] && sl.tag == tag_base + base + k) win++;
-                else key[k] = kEmpty;
             }
             u64 agg;
             u64 ex = block_exclusive_scan((u64)win, sm, &agg);
@@ -622,12 +644,15 @@ __global__ void __launch_bounds__(kThreads) select_kernel(IterCtl* __restrict__ 
             }
         }
     }
-    // the last block to finish runs the iteration end (after every write of this launch)
+    // the last block to finish runs the iteration end (after every write of this launch);
+    // blocks past the last tile never write, so only min(grid, tiles) blocks take part
+    const u32 parting = (u32)min((u64)gridDim.x, (active && c > 0) ? ntiles : (u64)1);
+    if (blockIdx.x >= parting) return;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         const u32 done = atomicAdd(&ctl->exit_ctr, 1u);
-        if (done == gridDim.x - 1) {
+        if (done == parting - 1) {
             __threadfence();
             ctl->exit_ctr = 0;
             if (a.last) end_of_iteration(ctl, plan, rm, history, cond, use_cond);

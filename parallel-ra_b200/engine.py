@@ -13,7 +13,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libra_b200.so")
+# RA_ENGINE_LIB: path of another build of the engine library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("RA_ENGINE_LIB") or os.path.join(HERE, "libra_b200.so")
 
 DELTA, FULL = 0, 1
 COPY, ACOPY, COPY_FILTER = 0, 1, 2
