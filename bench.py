@@ -49,10 +49,10 @@ WORKLOADS = {
 CPU_SAMPLE = (1 << 17, round(0.95 * (1 << 17)), 2)
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
-# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.75 / 1.81 / 1.76 over
+# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.79 / 1.81 / 1.83 over
 # three launches of the same graph family at 1/4 scale); bench's `traffic` is
 # this ratio times the algorithmic bytes of an average tc-er22 launch.
-TRAFFIC_PER_ALGO_BYTE = 1.77
+TRAFFIC_PER_ALGO_BYTE = 1.81
 
 
 def load_peaks():

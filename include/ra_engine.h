@@ -160,6 +160,10 @@ int ra_program_reset(ra_program* p);
  * RAM::check_for_fixed_point pushes (src/RAM/RA_tasks.cpp:1072-1085). */
 int ra_program_history(ra_program* p, uint64_t* out, uint64_t cap, uint64_t* len);
 int ra_program_stats(ra_program* p, ra_stats* out);
+/* Device time (microseconds) of every iteration of the last run that ran on
+ * the device-driven path, SCCs in execution order -- the Total_time column of
+ * RAM::execute_in_batches' per-iteration table (src/RAM/RA_tasks.cpp:1198-1235). */
+int ra_program_iteration_times(ra_program* p, double* out_us, uint64_t cap, uint64_t* len);
 
 /* relation::get_full_element_count / get_delta_element_count
  * (src/relation/balanced_hash_relation.h:183,206) */

@@ -124,6 +124,7 @@ struct ra_program {
     std::vector<Scc> sccs;
     std::vector<std::pair<int, int>> deps;
     std::vector<uint64_t> history;
+    std::vector<double> iter_us;  // device time of each device-driven iteration of the last run
     std::vector<std::pair<uint32_t, u64>> intern;   // (tag, next counter) -- LIE::intern_map
     int bits = 0;                 // packed bits per column for this run
     bool packed = false;          // loaded relations packed with `bits` (cleared by a new load)
@@ -980,9 +981,14 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
         p->status_cap = st_need;
     }
     if (hist_cap > p->dhist_cap) {
+        // layout: hist_cap (sum_delta, sum_full) pairs, then hist_cap iteration end times
         u64* nh;
-        dev_alloc(p, &nh, 2 * hist_cap);
-        if (p->dhist) CK(cudaMemcpyAsync(nh, p->dhist, 2 * p->dhist_cap * 8, cudaMemcpyDeviceToDevice, p->stream));
+        dev_alloc(p, &nh, 3 * hist_cap);
+        if (p->dhist) {
+            CK(cudaMemcpyAsync(nh, p->dhist, 2 * p->dhist_cap * 8, cudaMemcpyDeviceToDevice, p->stream));
+            CK(cudaMemcpyAsync(nh + 2 * hist_cap, p->dhist + 2 * p->dhist_cap, p->dhist_cap * 8,
+                               cudaMemcpyDeviceToDevice, p->stream));
+        }
         dev_free(p, &p->dhist);
         p->dhist = nh;
         p->dhist_cap = hist_cap;
@@ -991,6 +997,7 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     pl.cand_cap = p->dcand_cap;
     pl.stage_cap = ref ? p->stage_cap : ~0ull;
     pl.hist_cap = p->dhist_cap;
+    p->hctl->time_cap = p->dhist_cap;
     for (int sl = 0; sl < pl.n_rels; sl++) {
         Relation& r = p->rels[d.rel_of_slot[sl]];
         pl.log_cap[sl] = r.cap;
@@ -1170,6 +1177,9 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     dev_size_buffers(p, d, std::max<u64>({p->dcand_cap, 1u << 22, 2 * outer0}),
                      std::max<u64>({p->stage_cap, 1u << 22, 2 * outer0}), std::max<u64>(p->dhist_cap, 1u << 12));
     CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+    CK(cudaMemcpyAsync(&p->ctl->time_cap, &p->hctl->time_cap, 8, cudaMemcpyHostToDevice, p->stream));
+    scc_start_kernel<<<1, 1, 0, p->stream>>>(p->ctl);
+    LAUNCHED();
 
     int body_kernels = 0;
     const bool graph_mode = p->use_graphs && !p->kernel_events && s.fixpoint;
@@ -1265,9 +1275,17 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     }
     // results back into the host-side relation records
     std::vector<u64> hist(2 * h.hist_n);
-    if (h.hist_n) {
-        CK(cudaMemcpyAsync(hist.data(), p->dhist, 2 * h.hist_n * 8, cudaMemcpyDeviceToHost, p->stream));
-        CK(cudaStreamSynchronize(p->stream));
+    const u64 nt = std::min<u64>(h.iteration, p->dhist_cap);
+    std::vector<u64> ends(nt);
+    if (h.hist_n) CK(cudaMemcpyAsync(hist.data(), p->dhist, 2 * h.hist_n * 8, cudaMemcpyDeviceToHost, p->stream));
+    if (nt) CK(cudaMemcpyAsync(ends.data(), p->dhist + 2 * p->dhist_cap, nt * 8, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    {
+        u64 prev = h.t_start;
+        for (u64 i = 0; i < nt; i++) {
+            p->iter_us.push_back(ends[i] >= prev ? (double)(ends[i] - prev) / 1e3 : 0.0);
+            prev = ends[i];
+        }
     }
     for (int sl = 0; sl < pl.n_rels; sl++) {
         Relation& r = p->rels[d.rel_of_slot[sl]];
@@ -1388,6 +1406,7 @@ void reset_state(ra_program* p)
     }
     for (Scc& s : p->sccs) s.done = false;
     p->history.clear();
+    p->iter_us.clear();
     p->intern.clear();
     p->executed = false;
     p->running = false;
@@ -1808,6 +1827,14 @@ int ra_program_history(ra_program* p, uint64_t* out, uint64_t cap, uint64_t* len
     return guard(p, [&] {
         if (len) *len = p->history.size();
         if (out) std::memcpy(out, p->history.data(), std::min<u64>(cap, p->history.size()) * 8);
+    });
+}
+
+int ra_program_iteration_times(ra_program* p, double* out_us, uint64_t cap, uint64_t* len)
+{
+    return guard(p, [&] {
+        if (len) *len = p->iter_us.size();
+        if (out_us) std::memcpy(out_us, p->iter_us.data(), std::min<u64>(cap, p->iter_us.size()) * 8);
     });
 }
 

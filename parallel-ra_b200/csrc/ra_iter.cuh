@@ -51,6 +51,8 @@ struct IterCtl {
     u64 hist_n;             // (sum_delta, sum_full) pairs recorded
     u64 new_tuples, candidates, outer_rows;
     u64 runs[kMaxSccRels];  // non-empty deltas moved into full (sorted runs added)
+    u64 t_start;                    // %globaltimer when the SCC started (ns)
+    u64 time_cap;                   // entries of the per-iteration end-time buffer
     u32 tile_ctr[2 * kTileSlots];   // two banks: iteration k uses bank k & 1
     u32 exit_ctr;                   // blocks of the running select launch that have finished
     u32 flags;
@@ -476,6 +478,15 @@ struct SccRelMap {
     int rules_in[kMaxSccRels][kMaxSccRules];
 };
 
+__device__ __forceinline__ u64 global_ns()
+{
+    u64 t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// history holds plan.hist_cap (sum_delta, sum_full) pairs, then time_cap
+// per-iteration end times (%globaltimer, ns)
 __device__ void end_of_iteration(IterCtl* __restrict__ ctl, const SccPlan& plan, const SccRelMap& rm,
                                  u64* __restrict__ history, cudaGraphConditionalHandle cond, int use_cond)
 {
@@ -508,6 +519,7 @@ __device__ void end_of_iteration(IterCtl* __restrict__ ctl, const SccPlan& plan,
         for (int r = 0; r < plan.n_rules; r++) cands += ctl->cand_n[r];
         ctl->candidates += cands;
         ctl->new_tuples += added;
+        if (ctl->iteration < ctl->time_cap) history[2 * plan.hist_cap + ctl->iteration] = global_ns();
         ctl->iteration++;
         ctl->epoch++;
         ctl->batch_pos++;
@@ -800,6 +812,8 @@ __global__ void __launch_bounds__(kThreads) sort_pass_kernel(IterCtl* __restrict
         __syncthreads();
     }
 }
+
+__global__ void scc_start_kernel(IterCtl* __restrict__ ctl) { ctl->t_start = global_ns(); }
 
 // ---------------------------------------------------------------------------
 // iteration end as its own launch (reference id order: after the sort passes)

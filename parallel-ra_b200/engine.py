@@ -26,7 +26,7 @@ EXPORTS = (
     "ra_program_set_id_order", "ra_program_set_launch_timing",
     "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
-    "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats",
+    "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats", "ra_program_iteration_times",
     "ra_relation_counts", "ra_relation_dump_full", "ra_rows_distinct_noalloc", "ra_status_string", "ra_last_error",
 )
 
@@ -81,6 +81,7 @@ def lib():
         L.ra_program_reset.argtypes = [P]
         L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
+        L.ra_program_iteration_times.argtypes = [P, C.POINTER(C.c_double), C.c_uint64, u64p]
         L.ra_relation_counts.argtypes = [P, C.c_int, u64p, u64p]
         L.ra_relation_dump_full.argtypes = [P, C.c_int, u64p, C.c_uint64, u64p]
         L.ra_rows_distinct_noalloc.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -203,6 +204,14 @@ class Program:
         s = Stats()
         self._ck(self._L.ra_program_stats(self._p, C.byref(s)), "stats")
         return s
+
+    def iteration_times_us(self):
+        """Device time of each device-driven iteration of the last run (microseconds)."""
+        n = C.c_uint64()
+        self._ck(self._L.ra_program_iteration_times(self._p, None, 0, C.byref(n)), "iteration_times")
+        buf = (C.c_double * max(n.value, 1))()
+        self._ck(self._L.ra_program_iteration_times(self._p, buf, n.value, C.byref(n)), "iteration_times")
+        return list(buf)[:n.value]
 
     def counts(self, rel):
         f, d = C.c_uint64(), C.c_uint64()
