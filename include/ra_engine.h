@@ -95,6 +95,8 @@ typedef struct ra_stats {
     uint64_t graph_builds;      /* CUDA graphs captured + instantiated by the run */
     double graph_build_ms;      /* host time spent building them */
     uint64_t regrows;           /* buffer regrowths (iteration retried) */
+    uint64_t device_bytes;      /* device memory the program holds after the run */
+    uint64_t device_bytes_peak; /* most device memory it held during the run */
 } ra_stats;
 
 /* Create a program on CUDA device `device`.  Replaces the per-rank set-up of
@@ -173,6 +175,32 @@ int ra_relation_counts(ra_program* p, int rel, uint64_t* full, uint64_t* delta);
  * Writes min(cap_rows, count) rows to host memory. */
 int ra_relation_dump_full(ra_program* p, int rel, uint64_t* host_rows, uint64_t cap_rows,
                           uint64_t* rows_out);
+
+/* Batched instances (an extension; the reference runs one program instance per
+ * mpirun).  Several independent instances of one program run as a single
+ * program over their disjoint union: the caller rebases instance i's values by
+ * value_base[i] (strictly increasing; instance i owns the values
+ * [value_base[i], value_base[i+1]), the last one everything above its base).
+ * Joins match equal values only, so no tuple crosses instances and every
+ * iteration of the union is the same iteration of each instance.  Set before a
+ * run (n_instances = 0 switches accounting off); the engine then counts every
+ * iteration's new tuples per instance, inside the device's winner selection. */
+int ra_program_set_instances(ra_program* p, const uint64_t* value_base, uint32_t n_instances);
+/* Per-instance new-tuple counts of every iteration of the last run, SCCs in
+ * execution order: rows of n_instances counts, one row per iteration -- per
+ * instance the sum_delta that RAM::check_for_fixed_point pushes
+ * (src/RAM/RA_tasks.cpp:1072-1085) for batch size 1.  *rows = iterations
+ * recorded; min(cap_rows, *rows) rows are written.  RA_E_UNSUPPORTED when an
+ * SCC of the run took the host path, which keeps no per-instance counts. */
+int ra_program_instance_history(ra_program* p, uint64_t* out, uint64_t cap_rows, uint64_t* rows);
+/* Per-instance row count and order-independent digest of a relation's full
+ * version: counts[i] and digests[i] (n_instances entries each, or one entry
+ * when no instances are set) cover the rows whose column 0 lies in instance
+ * i's range.  The digest is a sum over rows of a hash of the data columns
+ * minus the instance base (ids excluded), so it does not depend on the packing
+ * width, the row order or the other instances: a batched run's digest of
+ * instance i equals a plain run's digest of that instance alone. */
+int ra_relation_instance_summary(ra_program* p, int rel, uint64_t* counts, uint64_t* digests);
 
 /* Largest row count ra_rows_distinct_noalloc accepts. */
 #define RA_NOALLOC_MAX_ROWS (1u << 17)

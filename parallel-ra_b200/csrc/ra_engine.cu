@@ -26,6 +26,7 @@
 #include <atomic>
 #include <functional>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 using namespace ra;
@@ -106,8 +107,10 @@ struct Relation {
     // CSR index on the join key, for full (version-stamped) and delta
     u64* csr_full = nullptr;
     u64 csr_full_version = ~0ull;
+    u64 csr_full_cap = 0;          // entries (2^join-key-bits + 1 of the run that built it)
     u64* csr_delta = nullptr;
     u64 csr_delta_version = ~0ull;
+    u64 csr_delta_cap = 0;
     // newt staging for the running iteration
     u64 newt_n = 0;
 };
@@ -134,6 +137,8 @@ struct ra_program {
     u64 epoch = 0;
     std::string err;
     ra_stats stats{};
+    std::unordered_map<void*, u64> alloc_bytes;   // live device allocations
+    u64 live_bytes = 0;
     // scratch
     u64* cand = nullptr;
     u64 cand_cap = 0;
@@ -175,6 +180,14 @@ struct ra_program {
     u64* sort_v[2] = {};
     u64* status = nullptr;
     u64 status_cap = 0;
+    // instances (batched programs): instance i owns values [inst_base_h[i], inst_base_h[i + 1])
+    std::vector<u64> inst_base_h;  // n_inst + 1 entries, the last ~0
+    u64* dinst_base = nullptr;
+    u32 n_inst = 0;
+    u64* dinst_new = nullptr;      // [iteration][instance] new tuples of the running SCC
+    u64 inst_rows_cap = 0;
+    std::vector<u64> inst_hist;    // per iteration of the run: n_inst new-tuple counts
+    bool inst_hist_ok = true;      // false once an SCC ran without instance accounting
     u64* dhist = nullptr;
     u64 dhist_cap = 0;
     bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
@@ -211,12 +224,24 @@ void dev_alloc(ra_program* p, T** ptr, u64 count)
     if (count == 0) count = 1;
     CK(cudaMallocAsync(&q, count * sizeof(T), p->stream));
     *ptr = (T*)q;
+    p->alloc_bytes[q] = count * sizeof(T);
+    p->live_bytes += count * sizeof(T);
+    p->stats.device_bytes = p->live_bytes;
+    p->stats.device_bytes_peak = std::max<uint64_t>(p->stats.device_bytes_peak, p->live_bytes);
 }
 
 template <typename T>
 void dev_free(ra_program* p, T** ptr)
 {
-    if (*ptr) cudaFreeAsync(*ptr, p->stream);
+    if (*ptr) {
+        cudaFreeAsync(*ptr, p->stream);
+        auto it = p->alloc_bytes.find((void*)*ptr);
+        if (it != p->alloc_bytes.end()) {
+            p->live_bytes -= it->second;
+            p->alloc_bytes.erase(it);
+        }
+        p->stats.device_bytes = p->live_bytes;
+    }
     *ptr = nullptr;
 }
 
@@ -458,10 +483,16 @@ const u64* version_csr(ra_program* p, Relation& r, int ver)
              r.name.c_str(), jbits);
     u64** slot = (ver == RA_DELTA) ? &r.csr_delta : &r.csr_full;
     u64* stamp = (ver == RA_DELTA) ? &r.csr_delta_version : &r.csr_full_version;
+    u64* cap = (ver == RA_DELTA) ? &r.csr_delta_cap : &r.csr_full_cap;
     u64 want = (ver == RA_DELTA) ? r.delta_version : r.full_version;
     if (*slot && *stamp == want) return *slot;
+    // the key width changes with the values loaded: a reloaded program may need a larger index
     const u64 nk = (1ull << jbits) + 1;
-    if (!*slot) dev_alloc(p, slot, nk);
+    if (*cap < nk) {
+        dev_free(p, slot);
+        dev_alloc(p, slot, nk);
+        *cap = nk;
+    }
     const u64 *k, *v;
     u64 n;
     version_rows(p, r, ver, &k, &v, &n);
@@ -1005,6 +1036,20 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     }
 }
 
+// Instance matrix with room for `rows` iterations; keeps the rows already written.
+void size_instance_rows(ra_program* p, u64 rows)
+{
+    if (!p->n_inst || rows <= p->inst_rows_cap) return;
+    u64* nm;
+    dev_alloc(p, &nm, rows * p->n_inst);
+    CK(cudaMemsetAsync(nm, 0, rows * p->n_inst * 8, p->stream));
+    if (p->dinst_new)
+        CK(cudaMemcpyAsync(nm, p->dinst_new, p->inst_rows_cap * p->n_inst * 8, cudaMemcpyDeviceToDevice, p->stream));
+    dev_free(p, &p->dinst_new);
+    p->dinst_new = nm;
+    p->inst_rows_cap = rows;
+}
+
 // per-launch events (diagnostic mode only; never inside a graph capture)
 struct PhaseTimer {
     ra_program* p;
@@ -1058,8 +1103,14 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         a.dst_keys = ref ? p->stage_k[r.out_slot] : out.keys;
         a.dst_ids = ref ? p->stage_v[r.out_slot] : out.ids;
         a.passes = ref ? d.passes[r.out_slot] : 0;
-        a.log_cap = out.cap;
         a.stage_cap = p->stage_cap;
+        if (p->n_inst) {
+            a.inst_base = p->dinst_base;
+            a.n_inst = p->n_inst;
+            a.inst_shift = (int)(out.arity - 1) * p->bits;
+            a.inst_new = p->dinst_new;
+            a.inst_iter_cap = p->inst_rows_cap;
+        }
         select_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, p->dloser, p->status, slot++,
                                                      p->dhist, cond, use_cond);
         launches++;
@@ -1124,6 +1175,10 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
     put(&p->id_order, sizeof p->id_order);
     put(&p->stage_cap, sizeof p->stage_cap);
     put(&p->dcand_cap, sizeof p->dcand_cap);
+    const void* inst[2] = {p->dinst_base, p->dinst_new};
+    put(inst, sizeof inst);
+    put(&p->n_inst, sizeof p->n_inst);
+    put(&p->inst_rows_cap, sizeof p->inst_rows_cap);
     return sig;
 }
 
@@ -1178,6 +1233,10 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                      std::max<u64>({p->stage_cap, 1u << 22, 2 * outer0}), std::max<u64>(p->dhist_cap, 1u << 12));
     CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
     CK(cudaMemcpyAsync(&p->ctl->time_cap, &p->hctl->time_cap, 8, cudaMemcpyHostToDevice, p->stream));
+    if (p->n_inst) {
+        size_instance_rows(p, 256);
+        CK(cudaMemsetAsync(p->dinst_new, 0, p->inst_rows_cap * p->n_inst * 8, p->stream));
+    }
     scc_start_kernel<<<1, 1, 0, p->stream>>>(p->ctl);
     LAUNCHED();
 
@@ -1259,6 +1318,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             dev_size_buffers(p, d, replay ? std::max(p->dcand_cap, 2 * total) : p->dcand_cap,
                              replay ? std::max(p->stage_cap, 2 * stage_need) : p->stage_cap,
                              h.hist_n >= p->dhist_cap ? 2 * p->dhist_cap : p->dhist_cap);
+            if (p->n_inst && h.iteration >= p->inst_rows_cap) size_instance_rows(p, 2 * p->inst_rows_cap);
             h.flags = 0;
             h.exit_ctr = 0;
             if (replay)
@@ -1279,6 +1339,12 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     std::vector<u64> ends(nt);
     if (h.hist_n) CK(cudaMemcpyAsync(hist.data(), p->dhist, 2 * h.hist_n * 8, cudaMemcpyDeviceToHost, p->stream));
     if (nt) CK(cudaMemcpyAsync(ends.data(), p->dhist + 2 * p->dhist_cap, nt * 8, cudaMemcpyDeviceToHost, p->stream));
+    if (p->n_inst && h.iteration) {
+        const size_t at = p->inst_hist.size();
+        p->inst_hist.resize(at + (size_t)h.iteration * p->n_inst);
+        CK(cudaMemcpyAsync(p->inst_hist.data() + at, p->dinst_new, (size_t)h.iteration * p->n_inst * 8,
+                           cudaMemcpyDeviceToHost, p->stream));
+    }
     CK(cudaStreamSynchronize(p->stream));
     {
         u64 prev = h.t_start;
@@ -1335,6 +1401,7 @@ void run_scc(ra_program* p, Scc& s)
             return;
         }
     }
+    p->inst_hist_ok = false;   // the host path keeps no per-instance counts
     std::vector<uint64_t> hist;
     for (;;) {
         uint32_t b = p->batch_size;
@@ -1387,7 +1454,7 @@ void free_relation_state(ra_program* p, Relation& r)
     dev_free(p, &r.vids);
     dev_free(p, &r.csr_full);
     dev_free(p, &r.csr_delta);
-    r.cap = r.seen_cap = r.seen_n = r.v_cap = 0;
+    r.cap = r.seen_cap = r.seen_n = r.v_cap = r.csr_full_cap = r.csr_delta_cap = 0;
     r.v_version = r.csr_full_version = r.csr_delta_version = ~0ull;
     r.full_n = r.delta_n = r.newt_n = 0;
 }
@@ -1407,6 +1474,8 @@ void reset_state(ra_program* p)
     for (Scc& s : p->sccs) s.done = false;
     p->history.clear();
     p->iter_us.clear();
+    p->inst_hist.clear();
+    p->inst_hist_ok = true;
     p->intern.clear();
     p->executed = false;
     p->running = false;
@@ -1417,6 +1486,7 @@ void begin_run(ra_program* p)
 {
     if (p->executed || p->running) reset_state(p);
     p->stats = ra_stats{};
+    p->stats.device_bytes = p->stats.device_bytes_peak = p->live_bytes;
     for (auto& e : p->dedup_events) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
@@ -1604,6 +1674,8 @@ int ra_program_destroy(ra_program* p)
     }
     dev_free(p, &p->status);
     dev_free(p, &p->dhist);
+    dev_free(p, &p->dinst_base);
+    dev_free(p, &p->dinst_new);
     for (Scc& sc : p->sccs) drop_graph(sc);
     for (auto& e : p->dedup_events) {
         cudaEventDestroy(e.first);
@@ -1835,6 +1907,64 @@ int ra_program_iteration_times(ra_program* p, double* out_us, uint64_t cap, uint
     return guard(p, [&] {
         if (len) *len = p->iter_us.size();
         if (out_us) std::memcpy(out_us, p->iter_us.data(), std::min<u64>(cap, p->iter_us.size()) * 8);
+    });
+}
+
+int ra_program_set_instances(ra_program* p, const uint64_t* value_base, uint32_t n_instances)
+{
+    return guard(p, [&] {
+        if (p->running) fail(p, RA_E_STATE, "set_instances during a run");
+        if (n_instances && !value_base) fail(p, RA_E_BADARG, "null value_base");
+        for (uint32_t i = 1; i < n_instances; i++)
+            if (value_base[i] <= value_base[i - 1]) fail(p, RA_E_BADARG, "value_base must increase strictly");
+        dev_free(p, &p->dinst_base);
+        dev_free(p, &p->dinst_new);
+        p->inst_rows_cap = 0;
+        p->inst_base_h.clear();
+        p->n_inst = n_instances;
+        p->inst_hist.clear();
+        if (!n_instances) return;
+        p->inst_base_h.assign(value_base, value_base + n_instances);
+        p->inst_base_h.push_back(~0ull);
+        dev_alloc(p, &p->dinst_base, n_instances + 1);
+        CK(cudaMemcpyAsync(p->dinst_base, p->inst_base_h.data(), (n_instances + 1) * 8, cudaMemcpyHostToDevice,
+                           p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+    });
+}
+
+int ra_program_instance_history(ra_program* p, uint64_t* out, uint64_t cap_rows, uint64_t* rows)
+{
+    return guard(p, [&] {
+        if (!p->n_inst) fail(p, RA_E_STATE, "no instances set");
+        if (!p->inst_hist_ok) fail(p, RA_E_UNSUPPORTED, "an SCC of the run kept no per-instance counts");
+        const u64 n = p->inst_hist.size() / p->n_inst;
+        if (rows) *rows = n;
+        if (out) std::memcpy(out, p->inst_hist.data(), std::min<u64>(cap_rows, n) * p->n_inst * 8);
+    });
+}
+
+int ra_relation_instance_summary(ra_program* p, int rel, uint64_t* counts, uint64_t* digests)
+{
+    return guard(p, [&] {
+        Relation& r = rel_at(p, rel);
+        if (!p->executed) fail(p, RA_E_STATE, "summary before execute");
+        if (!counts || !digests) fail(p, RA_E_BADARG, "null output");
+        const u64 m = std::max<u32>(p->n_inst, 1);
+        u64* acc;
+        dev_alloc(p, &acc, 2 * m);
+        CK(cudaMemsetAsync(acc, 0, 2 * m * 8, p->stream));
+        if (r.full_n) {
+            instance_summary_kernel<<<grid_for((r.full_n + kSummaryRowsPerLane - 1) / kSummaryRowsPerLane), kThreads, 0,
+                                      p->stream>>>(
+                r.keys, r.full_n, (int)r.arity, p->bits, p->n_inst ? p->dinst_base : nullptr, p->n_inst, acc,
+                acc + m);
+            LAUNCHED();
+        }
+        CK(cudaMemcpyAsync(counts, acc, m * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaMemcpyAsync(digests, acc + m, m * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        dev_free(p, &acc);
     });
 }
 

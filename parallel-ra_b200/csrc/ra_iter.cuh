@@ -557,9 +557,26 @@ struct SelectArgs {
     u64* dst_ids;
     int to_log;
     int passes;               // digit histograms to accumulate (reference ids)
-    u64 log_cap;              // rows the output relation's log holds
     u64 stage_cap;
+    // instance accounting (batched programs): instance i owns values [inst_base[i], inst_base[i+1])
+    const u64* inst_base;     // n_inst + 1 entries, or null
+    u32 n_inst;
+    int inst_shift;           // bit offset of column 0 in the output relation's key
+    u64* inst_new;            // [iteration][instance] counts of new tuples
+    u64 inst_iter_cap;
 };
+
+// instance owning value v (inst_base sorted, n + 1 entries)
+__device__ __forceinline__ u32 instance_of(const u64* __restrict__ base, u32 n, u64 v)
+{
+    u32 lo = 0, hi = n;   // base[lo] <= v < base[hi]
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (__ldg(&base[mid]) <= v) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
 
 __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
                                                           SelectArgs a, const u64* __restrict__ cand,
@@ -577,12 +594,18 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
     const int out = plan.rule_out[rule], tslot = plan.rule_tag[rule];
     bool active = ctl->flags == 0;
     if (active) {
-        // room for every candidate of every rule into this relation, checked before any write
-        u64 incoming = 0;
-        for (int q = 0; q < rm.n_rules_in[out]; q++) incoming += ctl->cand_n[rm.rules_in[out][q]];
-        // the new delta lands in the log either way (directly, or via staging + sort)
-        const bool over = ctl->full_n[out] + ctl->delta_n[out] + incoming > a.log_cap ||
-                          (!a.to_log && incoming > a.stage_cap);
+        // Room for every candidate of every rule of the iteration, checked by every select
+        // before any write, so that an iteration either writes all its winners or none
+        // (a replay then never counts a winner twice).  The new delta lands in the log
+        // either way (directly, or via staging + sort).
+        bool over = a.inst_base && ctl->iteration >= a.inst_iter_cap;
+        for (int s = 0; s < plan.n_rels; s++) {
+            u64 incoming = 0;
+            for (int q = 0; q < rm.n_rules_in[s]; q++) incoming += ctl->cand_n[rm.rules_in[s][q]];
+            if (!incoming) continue;
+            over = over || ctl->full_n[s] + ctl->delta_n[s] + incoming > plan.log_cap[s] ||
+                   (!a.to_log && incoming > a.stage_cap);
+        }
         if (over) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
             active = false;
@@ -644,6 +667,17 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
                 for (int ps = 0; ps < a.passes; ps++)
                     atomicAdd(&s_hist[ps][(key[k] >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
                 r++;
+            }
+            if (a.inst_base) {
+                u64* row = a.inst_new + ctl->iteration * a.n_inst;
+#pragma unroll
+                for (int k = 0; k < kSelIpt; k++) {
+                    const bool v = key[k] != kEmpty;
+                    const u32 inst = v ? instance_of(a.inst_base, a.n_inst, key[k] >> a.inst_shift)
+                                       : (0x80000000u | (u32)threadIdx.x);
+                    const u32 peers = __match_any_sync(0xffffffffu, inst);
+                    if (v && (peers & lanemask_lt()) == 0) atomicAdd(&row[inst], (u64)__popc(peers));
+                }
             }
             if (tile == ntiles - 1 && threadIdx.x == 0) ctl->win_n[rule] = s_prefix + agg;
             __syncthreads();
@@ -814,6 +848,80 @@ __global__ void __launch_bounds__(kThreads) sort_pass_kernel(IterCtl* __restrict
 }
 
 __global__ void scc_start_kernel(IterCtl* __restrict__ ctl) { ctl->t_start = global_ns(); }
+
+// Order-independent digest of a tuple's data columns: depends only on the
+// column values (not on the packing width), so runs with different widths agree.
+__device__ __forceinline__ u64 tuple_digest(const u64* cols, int arity)
+{
+    u64 h = 0x9e3779b97f4a7c15ull * (u64)arity;
+    for (int c = 0; c < arity; c++) h = mix64(h ^ (cols[c] + 0x632be59bd9b4e019ull * (u64)(c + 1)));
+    return h;
+}
+
+// Per-instance count and digest (sum of tuple digests, values rebased to the
+// instance) of packed rows.  Each warp walks a contiguous segment of rows
+// (coalesced), every lane keeps a running (count, digest) for the instance of
+// its last rows and flushes it when the instance changes; relation logs hold
+// each instance's rows in long runs, so flushes are rare.  Up to
+// kSummarySmemInst instances accumulate in shared memory first.
+constexpr u32 kSummarySmemInst = 1024;
+constexpr int kSummaryRowsPerLane = 16;
+
+__global__ void __launch_bounds__(kThreads) instance_summary_kernel(
+    const u64* __restrict__ keys, u64 n, int arity, int bits, const u64* __restrict__ base, u32 n_inst,
+    u64* __restrict__ counts, u64* __restrict__ digests)
+{
+    __shared__ u64 s_cnt[kSummarySmemInst];
+    __shared__ u64 s_dig[kSummarySmemInst];
+    const u32 m = base ? n_inst : 1;
+    const bool in_smem = m <= kSummarySmemInst;
+    if (in_smem)
+        for (u32 i = threadIdx.x; i < m; i += blockDim.x) s_cnt[i] = s_dig[i] = 0;
+    __syncthreads();
+    u32 cur = 0xffffffffu;
+    u64 c = 0, dsum = 0;
+    auto flush = [&]() {
+        if (!c) return;
+        if (in_smem) {
+            atomicAdd((unsigned long long*)&s_cnt[cur], (unsigned long long)c);
+            atomicAdd((unsigned long long*)&s_dig[cur], (unsigned long long)dsum);
+        } else {
+            atomicAdd((unsigned long long*)&counts[cur], (unsigned long long)c);
+            atomicAdd((unsigned long long*)&digests[cur], (unsigned long long)dsum);
+        }
+        c = 0;
+        dsum = 0;
+    };
+    const int lane = threadIdx.x & 31;
+    const u64 seg = 32ull * kSummaryRowsPerLane;
+    const u64 warps = (u64)gridDim.x * (blockDim.x >> 5);
+    for (u64 w = (u64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w * seg < n; w += warps) {
+        for (int j = 0; j < kSummaryRowsPerLane; j++) {
+            const u64 i = w * seg + (u64)j * 32 + lane;
+            if (i >= n) break;
+            const u64 k = keys[i];
+            u64 cols[kMaxArity];
+            for (int q = 0; q < arity; q++) cols[q] = column_of(k, arity, q, bits);
+            const u32 inst = base ? instance_of(base, n_inst, cols[0]) : 0;
+            if (inst != cur) {
+                flush();
+                cur = inst;
+            }
+            const u64 b = base ? __ldg(&base[inst]) : 0;
+            for (int q = 0; q < arity; q++) cols[q] -= b;
+            c++;
+            dsum += tuple_digest(cols, arity);
+        }
+    }
+    flush();
+    if (!in_smem) return;
+    __syncthreads();
+    for (u32 i = threadIdx.x; i < m; i += blockDim.x)
+        if (s_cnt[i]) {
+            atomicAdd((unsigned long long*)&counts[i], (unsigned long long)s_cnt[i]);
+            atomicAdd((unsigned long long*)&digests[i], (unsigned long long)s_dig[i]);
+        }
+}
 
 // ---------------------------------------------------------------------------
 // iteration end as its own launch (reference id order: after the sort passes)

@@ -28,6 +28,7 @@ EXPORTS = (
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
     "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats", "ra_program_iteration_times",
     "ra_relation_counts", "ra_relation_dump_full", "ra_rows_distinct_noalloc", "ra_status_string", "ra_last_error",
+    "ra_program_set_instances", "ra_program_instance_history", "ra_relation_instance_summary",
 )
 
 
@@ -43,7 +44,8 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_uint64), ("fixpoint_ms", C.c_double), ("dedup_ms", C.c_double),
         ("dedup_launches", C.c_uint64), ("dedup_bytes", C.c_uint64), ("value_bits", C.c_uint32),
         ("reserved", C.c_uint32), ("phase_ms", C.c_double * 6), ("graph_builds", C.c_uint64),
-        ("graph_build_ms", C.c_double), ("regrows", C.c_uint64),
+        ("graph_build_ms", C.c_double), ("regrows", C.c_uint64), ("device_bytes", C.c_uint64),
+        ("device_bytes_peak", C.c_uint64),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 
@@ -84,6 +86,9 @@ def lib():
         L.ra_program_iteration_times.argtypes = [P, C.POINTER(C.c_double), C.c_uint64, u64p]
         L.ra_relation_counts.argtypes = [P, C.c_int, u64p, u64p]
         L.ra_relation_dump_full.argtypes = [P, C.c_int, u64p, C.c_uint64, u64p]
+        L.ra_program_set_instances.argtypes = [P, u64p, C.c_uint32]
+        L.ra_program_instance_history.argtypes = [P, u64p, C.c_uint64, u64p]
+        L.ra_relation_instance_summary.argtypes = [P, C.c_int, u64p, u64p]
         L.ra_rows_distinct_noalloc.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ra_status_string.argtypes = [C.c_int]
         L.ra_status_string.restype = C.c_char_p
@@ -108,6 +113,7 @@ class Program:
             raise RAError(st, f"ra_program_create(device={device}): {self._L.ra_status_string(st).decode()}")
         self._p = h
         self._arity = {}
+        self._n_inst = 0
         if id_order is not None:
             self.set_id_order(id_order)
 
@@ -229,3 +235,27 @@ class Program:
         got = C.c_uint64()
         self._ck(self._L.ra_relation_dump_full(self._p, rel, _u64(buf), n, C.byref(got)), "dump_full")
         return buf[:got.value]
+
+    def set_instances(self, value_base):
+        """Declare the instances of a batched run (value_base[i]: first value of instance i)."""
+        vb = np.ascontiguousarray(value_base, dtype=np.uint64)
+        self._n_inst = int(vb.size)
+        self._ck(self._L.ra_program_set_instances(self._p, _u64(vb) if vb.size else None, vb.size),
+                 "set_instances")
+
+    def instance_history(self) -> np.ndarray:
+        """New tuples per (iteration, instance) of the last run, shape (iterations, instances)."""
+        n = C.c_uint64()
+        self._ck(self._L.ra_program_instance_history(self._p, None, 0, C.byref(n)), "instance_history")
+        buf = np.zeros((max(n.value, 1), self._n_inst), dtype=np.uint64)
+        self._ck(self._L.ra_program_instance_history(self._p, _u64(buf), n.value, C.byref(n)), "instance_history")
+        return buf[:n.value]
+
+    def instance_summary(self, rel):
+        """Per-instance (row count, data digest) of a relation's full version, as two arrays."""
+        m = max(self._n_inst, 1)
+        counts = np.zeros(m, dtype=np.uint64)
+        digests = np.zeros(m, dtype=np.uint64)
+        self._ck(self._L.ra_relation_instance_summary(self._p, rel, _u64(counts), _u64(digests)),
+                 "instance_summary")
+        return counts, digests

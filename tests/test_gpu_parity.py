@@ -140,6 +140,20 @@ def test_rerun_after_reset_is_identical():
     assert np.array_equal(p.dump_full(rels["T"]), d1)
 
 
+def test_reload_with_wider_values():
+    """One program reloaded with inputs of growing value range (wider packed
+    columns, a larger join-key index) matches fresh programs and the oracle."""
+    p = P.Program(0)
+    rels = P.programs.PROGRAMS["tc"](p, np.empty((0, 3), dtype=np.uint64))
+    for n, m, seed in ((20, 30, 1), (300, 420, 2), (5000, 4500, 3), (40, 60, 4)):
+        rows = P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, seed))
+        p.load_rows(rels["G"], rows)
+        p.execute(1)
+        o, orels = run_oracle("tc", rows)
+        assert as_lists(p.history()) == as_lists(o.history()), n
+        assert np.array_equal(data_cols(p.dump_full(rels["T"])), data_cols(o.dump_full(orels["T"]))), n
+
+
 def test_emission_ids_are_deterministic_and_unique():
     rows = P.datagen.with_row_ids(P.datagen.erdos_renyi(3000, 4000, 12))
     a, ra = run_engine("tc", rows)
