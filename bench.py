@@ -122,7 +122,12 @@ class ClockSampler:
 def reference_sample_run(n, m, seed):
     """Run the reference (oracle/_ref/ref_driver) once; returns (tc_tuples, seconds, kind)."""
     import parallel_ra_b200 as P
-    rows = P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, seed))
+    return reference_rows_run(P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, seed)))
+
+
+def reference_rows_run(rows):
+    """TC of ``rows`` by the reference's CPU code; returns (tc_tuples, fixpoint seconds, kind)."""
+    import parallel_ra_b200 as P
     drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
     if os.path.exists(drv):
         with tempfile.TemporaryDirectory() as tmp:
@@ -149,6 +154,20 @@ def cpu_sample_desc():
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return None
+    if args.workload == "batched":
+        from parallel_ra_b200.batch import estimate_tuples
+        insts = batched_instances(BATCH_COUNT, BATCH_SEED)
+        total = sum(estimate_tuples("tc", r) for r in insts)
+        cb = batched_cpu_baseline(insts, total)
+        cb["sample"] += "; batch tuples from the closure-size estimate"
+        per_step = BATCH_COUNT / cb["value"]
+        return {"impl": "reference", "metric": "batched TC instances/s", "value": cb["value"],
+                "unit": "instances/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic", "config": {"workload": "batched", "instances": BATCH_COUNT,
+                                                "metric_family": METRIC_FAMILY},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "instances/s", "h2d_bytes_per_step": 0,
+                                            "d2h_bytes_per_step": 0}}
     n, m, s = CPU_SAMPLE
     vals = []
     for i in range(args.warmup + args.steps):
@@ -300,13 +319,181 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+BATCH_COUNT, BATCH_SEED = 8192, 1
+BATCH_SERIAL_SAMPLE = 512
+BATCH_CPU_SAMPLE = 12
+
+
+def batched_instances(count, seed):
+    """The batched workload: per-instance seeded ER graphs (datagen.batched_sizes)."""
+    import parallel_ra_b200 as P
+    return [P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, s)) for n, m, s in P.datagen.batched_sizes(count, seed)]
+
+
+def batched_cpu_baseline(insts, total_tuples):
+    """Reference CPU throughput on a bounded random sample of the batch (instances whose
+    closure is estimated below 5e6 tuples), converted to instances/s over the whole batch."""
+    from parallel_ra_b200.batch import estimate_tuples
+    rng = np.random.default_rng(7)
+    pool = [i for i in rng.permutation(len(insts)) if estimate_tuples("tc", insts[i]) < 5e6][:BATCH_CPU_SAMPLE]
+    tup = secs = 0.0
+    kind = "port"
+    for i in pool:
+        t, sec, kind = reference_rows_run(insts[i])
+        tup += t
+        secs += sec
+    tps = tup / secs
+    return {"value": len(insts) / (total_tuples / tps), "unit": "instances/s", "cores": 1, "kind": kind,
+            "tuples_per_s": tps,
+            "sample": f"{len(pool)} random instances of the batch with estimated closure < 5e6 tuples "
+                      f"({int(tup)} tuples, {secs:.1f} s fixpoint time); instances/s = batch size / "
+                      f"(batch tuples / sample tuples/s)"}
+
+
+def run_batched(args, rank, world, local_rank):
+    """8,192 independent TC instances (n log-uniform in [64, 16384], mean out-degree
+    uniform in [0.8, 2.0]) run as waves of rebased unions -- one CUDA-graph-driven
+    program per wave -- against plain one-instance-per-run executions."""
+    import torch
+    import parallel_ra_b200 as P
+    from parallel_ra_b200.batch import Runner, estimate_tuples, plan_waves, value_span
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    insts = batched_instances(BATCH_COUNT, BATCH_SEED + 1000 * rank)
+    est = np.array([estimate_tuples("tc", r) for r in insts])
+    order = np.argsort(-est, kind="stable")
+    free, _ = torch.cuda.mem_get_info(local_rank)
+    budget = args.wave_tuples or min(P.batch.WAVE_TUPLES, 0.5 * free / P.batch.BYTES_PER_TUPLE)
+    spans = [value_span(insts[i]) for i in order]
+    waves = [[int(order[j]) for j in w] for w in plan_waves(est[order], budget, max_values=(1 << 30) - 1,
+                                                             spans=spans)]
+    stream = torch.cuda.Stream()
+    runner = Runner("tc", local_rank)
+    runner.prog.set_stream(stream.cuda_stream)
+    # union rows of every wave resident in HBM before timing
+    staged = []
+    for w in waves:
+        union, base = Runner.union_rows([insts[i] for i in w])
+        staged.append((w, base, torch.from_numpy(union.view(np.int64)).to(dev), union.shape[0]))
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def one_pass():
+        res, launches, tuples, peak = {}, 0, 0, 0
+        for w, base, t, nrows in staged:
+            out = runner.run_wave_resident(base, t.data_ptr(), nrows)
+            st = runner.prog.stats()
+            launches += st.kernel_launches
+            peak = max(peak, st.device_bytes_peak)
+            for i, o in zip(w, out):
+                res[i] = o
+                tuples += o.counts["T"]
+        return res, launches, tuples, peak
+
+    for _ in range(args.warmup):
+        one_pass()
+    torch.cuda.synchronize()
+    step_ms, launches = [], 0
+    with ClockSampler(local_rank) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            res, launches, tuples, peak = one_pass()
+            b.record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(a.elapsed_time(b))
+    value = BATCH_COUNT * args.steps / (sum(step_ms) / 1e3)
+
+    # dominant kernel on the largest wave, with per-launch events
+    w, base, t, nrows = staged[0]
+    runner.prog.set_launch_timing(True)
+    runner.run_wave_resident(base, t.data_ptr(), nrows)
+    s2 = runner.prog.stats()
+    runner.prog.set_launch_timing(False)
+    peak_bw, peak_kind = load_peaks()
+    achieved = (s2.dedup_bytes / s2.dedup_launches) / ((s2.dedup_ms / s2.dedup_launches) / 1e3) / 1e9 \
+        if s2.dedup_launches else 0.0
+    roofline = {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak_bw, "unit": "GB/s",
+                "frac": achieved / peak_bw, "peak_kind": peak_kind,
+                "traffic": TRAFFIC_PER_ALGO_BYTE * s2.dedup_bytes / max(s2.dedup_launches, 1),
+                "traffic_note": "ncu DRAM read+write per algorithmic byte measured on tc-er20, times this "
+                                "wave's algorithmic bytes per launch",
+                "launches": int(s2.dedup_launches), "wave": "largest wave", "instances_in_wave": len(w)}
+    # end to end from host arrays: rebasing, upload, waves, per-instance results
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    res_e2e = {}
+    for w in waves:
+        out = runner.run_wave([insts[i] for i in w])
+        for i, o in zip(w, out):
+            res_e2e[i] = o
+        h2d += sum(insts[i].nbytes for i in w)
+        hist_rows = sum(it for _, it in runner._scc_blocks())
+        d2h += 8 * len(w) * (hist_rows + 2 * len(runner.rels))   # per-instance counts + (count, digest)
+    e2e_s = time.perf_counter() - t0
+    runner.close()          # release its buffers before the plain runs
+
+    # serial: plain one-instance-per-run executions of a random sample, each checked against its wave result
+    sample = np.random.default_rng(3).choice(BATCH_COUNT, BATCH_SERIAL_SAMPLE, replace=False)
+    plain = Runner("tc", local_rank)
+    plain.run_plain(insts[int(sample[0])])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mismatches = 0
+    for i in sample:
+        o = plain.run_plain(insts[int(i)])
+        mismatches += int(o.key() != res[int(i)].key() or o.key() != res_e2e[int(i)].key())
+    serial_s = time.perf_counter() - t0
+    plain.close()
+    if mismatches:
+        raise RuntimeError(f"{mismatches} batched instances differ from their plain runs")
+    serial_ips = BATCH_SERIAL_SAMPLE / serial_s
+
+    if rank != 0:
+        return None
+    iters = [sum(len(d) for d in res[i].deltas) for i in range(BATCH_COUNT)]
+    line = {
+        "metric": "batched TC instances/s", "value": value, "unit": "instances/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(step_ms) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "batched", "instances": BATCH_COUNT, "seed": BATCH_SEED,
+                   "sizes": "n log-uniform in [64, 16384], mean out-degree uniform in [0.8, 2.0]",
+                   "waves": len(waves), "wave_tuple_budget": budget, "tc_tuples": int(tuples),
+                   "tuples_per_s": tuples * args.steps / (sum(step_ms) / 1e3),
+                   "peak_device_bytes": int(peak), "max_instance_iterations": int(max(iters)),
+                   "l2": "flushed (256 MiB write) before every timed step; waves are larger than L2",
+                   "step": "every wave of the batch, union rows resident in HBM, per-instance results to host",
+                   "metric_family": METRIC_FAMILY},
+        "serial": {"value": serial_ips, "unit": "instances/s", "sample": int(BATCH_SERIAL_SAMPLE),
+                   "mode": "plain one-instance-per-run executions (one reused program) from host rows, "
+                           "random sample of the batch",
+                   "batched_e2e_over_serial": (BATCH_COUNT / e2e_s) / serial_ips,
+                   "bit_exact_mismatches": mismatches},
+        "clocks": clocks.summary(),
+        "e2e": {"value": BATCH_COUNT / e2e_s, "unit": "instances/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches), "roofline": roofline, "step_ms": step_ms,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = batched_cpu_baseline(insts, tuples)
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tc-er22", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="tc-er22", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--wave-tuples", type=float, default=0.0,
+                    help="batched: estimated derived tuples per wave (default: the autotuned size, "
+                         "capped by half the free device memory)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -323,6 +510,8 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.impl == "reference":
         line = run_reference_arm(args, rank, world)
+    elif args.workload == "batched":
+        line = run_batched(args, rank, world, local_rank)
     else:
         line = run_ours(args, rank, world, local_rank)
         if world > 1:

@@ -99,12 +99,35 @@ typedef struct ra_stats {
     uint64_t device_bytes_peak; /* most device memory it held during the run */
 } ra_stats;
 
+/* Runtime tuning of one program (no counterpart in the reference, whose
+ * B-tree/shmap indexes have no load factor).  Picked per machine by the
+ * autotuner (parallel-ra_b200/autotune.py); the defaults are its B200 choice.
+ *   seen_load_max       hash load factor: a relation's seen set (open addressing,
+ *                       power-of-two slots) is rebuilt larger before an
+ *                       iteration could push its load past this (0.1 .. 0.9)
+ *   seen_grow           a rebuilt seen set is sized for seen_grow x the tuples
+ *                       stored and arriving (1.1 .. 8): fewer rebuilds vs memory
+ *   log_growth          capacity factor when a relation's tuple log grows (1.1 .. 4)
+ *   join_blocks_per_sm  CTAs per SM of the fused join kernel (1 .. 16)
+ *   select_blocks_per_sm  CTAs per SM of the winner-selection kernel (1 .. 16) */
+typedef struct ra_tuning {
+    double seen_load_max;
+    double seen_grow;
+    double log_growth;
+    uint32_t join_blocks_per_sm;
+    uint32_t select_blocks_per_sm;
+} ra_tuning;
+
 /* Create a program on CUDA device `device`.  Replaces the per-rank set-up of
  * mpi_comm::create + LIE::LIE (src/comm/comm.cpp:22-30, src/lie/lie.h:67-81). */
 int ra_program_create(int device, ra_program** out);
 int ra_program_destroy(ra_program* p);
 /* Bind the program to an existing CUDA stream (cudaStream_t); 0 = engine's own. */
 int ra_program_set_stream(ra_program* p, void* stream);
+/* Read / replace the program's tuning (RA_E_BADARG outside the ranges above;
+ * RA_E_STATE during a run). */
+int ra_program_get_tuning(ra_program* p, ra_tuning* out);
+int ra_program_set_tuning(ra_program* p, const ra_tuning* t);
 /* Iterations per fixed-point check, LIE::set_batch_size (src/lie/lie.h:111). */
 int ra_program_set_batch_size(ra_program* p, uint32_t batch_size);
 /* RA_IDS_EMISSION or RA_IDS_REFERENCE (no counterpart in the reference, whose
@@ -156,6 +179,12 @@ int ra_program_execute(ra_program* p);
 int ra_program_run_next_scc(ra_program* p, int* scc_id);
 /* Return every relation to its loaded state so the program can run again. */
 int ra_program_reset(ra_program* p);
+/* Free the device memory a program keeps between runs (relation logs, seen
+ * sets, indexes, iteration scratch, captured graphs) -- the memory-return
+ * step of a long-lived server; loaded rows stay.  Ends the last run (its
+ * results are gone); the next run allocates afresh.  No reference
+ * counterpart: the reference frees its relations only at exit (~LIE). */
+int ra_program_release(ra_program* p);
 
 /* Per-SCC history in execution order, flattened as
  * [scc_id, n, (sum_delta, sum_full) x n] per SCC -- the values that

@@ -24,13 +24,16 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .engine import Program
+from .engine import Program, tuning_file
 from .programs import PROGRAMS
 
-# bytes of device memory per derived tuple at the peak of a run (log keys + ids
-# with doubling slack, seen-set slots at <= 0.65 load, candidate and loser-mark
-# buffers); wave sizing divides the memory budget by it
-BYTES_PER_TUPLE = 160
+# Device memory per derived tuple at the peak of a run (log keys + ids with
+# growth slack, seen-set slots at the tuned load, candidate and loser-mark
+# buffers) and the estimated derived tuples per wave: the autotuner's
+# measurements when it has run on this machine, else conservative defaults.
+_TUNED = tuning_file() or {}
+BYTES_PER_TUPLE = float(_TUNED.get("bytes_per_tuple", 160.0))
+WAVE_TUPLES = float(_TUNED.get("wave_tuples", 3e8))
 
 
 @dataclass
@@ -180,22 +183,31 @@ class Runner:
             res.digests[name] = int(d[0])
         return res
 
+    @staticmethod
+    def union_rows(rows_list):
+        """(union rows, value bases): instance i's data columns shifted by base[i]."""
+        k = len(rows_list)
+        spans = np.fromiter((value_span(r) for r in rows_list), dtype=np.uint64, count=k)
+        base = np.zeros(k, dtype=np.uint64)
+        if k > 1:
+            base[1:] = np.cumsum(spans[:-1])
+        if not k:
+            return np.empty((0, 3), dtype=np.uint64), base
+        union = np.concatenate(rows_list).astype(np.uint64, copy=False)
+        sizes = np.fromiter((r.shape[0] for r in rows_list), dtype=np.int64, count=k)
+        union[:, :-1] += np.repeat(base, sizes)[:, None]
+        return union, base
+
     def load_wave(self, rows_list) -> np.ndarray:
         """Rebase and concatenate the instances; declare them to the engine."""
-        spans = [value_span(r) for r in rows_list]
-        base = np.zeros(len(rows_list), dtype=np.uint64)
-        if len(rows_list) > 1:
-            base[1:] = np.cumsum(np.asarray(spans[:-1], dtype=np.uint64))
-        parts = []
-        for b, r in zip(base, rows_list):
-            q = r.copy()
-            q[:, :-1] += b
-            parts.append(q)
-        union = np.concatenate(parts) if parts else np.empty((0, 3), dtype=np.uint64)
-        self.prog.set_instances(base)
-        self._instances = len(rows_list)
+        union, base = self.union_rows(rows_list)
+        self.declare(base)
         self.prog.load_rows(self.rels[self.input], union)
         return base
+
+    def declare(self, base):
+        self.prog.set_instances(base)
+        self._instances = len(base)
 
     def collect_wave(self, n: int) -> list[InstanceResult]:
         hist = self.prog.instance_history()
@@ -204,14 +216,27 @@ class Runner:
         for _, iters in self._scc_blocks():
             blk = hist[at:at + iters]
             at += iters
+            # per instance: rows up to its last non-zero count (its own iterations)
+            nz = blk != 0
+            last = np.where(nz.any(axis=0), iters - 1 - np.argmax(nz[::-1], axis=0), -1) if iters else \
+                np.full(n, -1)
+            cols = blk.T.tolist()
             for i in range(n):
-                out[i].deltas.append(_strip(blk[:, i]))
+                out[i].deltas.append(cols[i][:last[i] + 1])
         for name, h in self.rels.items():
             c, d = self.prog.instance_summary(h)
+            c, d = c.tolist(), d.tolist()
             for i in range(n):
-                out[i].counts[name] = int(c[i])
-                out[i].digests[name] = int(d[i])
+                out[i].counts[name] = c[i]
+                out[i].digests[name] = d[i]
         return out
+
+    def run_wave_resident(self, base, dev_rows: int, nrows: int) -> list[InstanceResult]:
+        """A wave whose union rows (built by ``union_rows``) are already in device memory."""
+        self.declare(base)
+        self.prog.load_rows_device(self.rels[self.input], dev_rows, nrows)
+        self.prog.execute()
+        return self.collect_wave(len(base))
 
     def run_wave(self, rows_list) -> list[InstanceResult]:
         self.load_wave(rows_list)

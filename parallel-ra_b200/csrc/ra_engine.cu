@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -123,6 +124,7 @@ struct ra_program {
     bool own_stream = false;
     uint32_t batch_size = 1;
     int id_order = RA_IDS_EMISSION;
+    ra_tuning tune = {0.45, 4.0, 1.5, 4, 4};   // the autotuner's B200 choice (tuning.json)
     std::vector<Relation> rels;
     std::vector<Scc> sccs;
     std::vector<std::pair<int, int>> deps;
@@ -245,11 +247,12 @@ void dev_free(ra_program* p, T** ptr)
     *ptr = nullptr;
 }
 
-// grow a pair of u64 buffers to at least n elements (contents preserved when keep)
-void grow2(ra_program* p, u64** a, u64** b, u64* cap, u64 n, bool keep, u64 keep_n)
+// grow a pair of u64 buffers to at least n elements, capacity growth x n
+// (contents preserved when keep)
+void grow2(ra_program* p, u64** a, u64** b, u64* cap, u64 n, bool keep, u64 keep_n, double growth = 1.5)
 {
     if (n <= *cap) return;
-    u64 nc = std::max<u64>(n + n / 2, 1024);
+    u64 nc = std::max<u64>((u64)((double)n * growth), 1024);
     u64 *na, *nb;
     dev_alloc(p, &na, nc);
     dev_alloc(p, &nb, nc);
@@ -369,7 +372,7 @@ Relation& rel_at(ra_program* p, int rel)
 
 void ensure_log(ra_program* p, Relation& r, u64 n)
 {
-    grow2(p, &r.keys, &r.ids, &r.cap, n, true, r.full_n + r.delta_n + r.newt_n);
+    grow2(p, &r.keys, &r.ids, &r.cap, n, true, r.full_n + r.delta_n + r.newt_n, p->tune.log_growth);
 }
 
 // ---------------------------------------------------------------------------
@@ -509,10 +512,12 @@ const u64* version_csr(ra_program* p, Relation& r, int ver)
     return *slot;
 }
 
+// seen set with room for `need` keys at the tuned maximum load (slot count
+// rounded up to whole 128-byte lines)
 void build_seen(ra_program* p, Relation& r, u64 need)
 {
-    u64 want = 1024;
-    while (want < 2 * need) want <<= 1;
+    u64 want = std::max<u64>((u64)std::ceil((double)need / p->tune.seen_load_max), 1024);
+    want = (want + 7) & ~7ull;
     if (r.seen && r.seen_cap >= want && !r.seen_dirty) return;
     if (!r.seen || r.seen_cap < want) {
         dev_free(p, &r.seen);
@@ -525,7 +530,7 @@ void build_seen(ra_program* p, Relation& r, u64 need)
     u64 n = r.full_n + r.delta_n;   // every stored tuple; newt is empty between iterations
     CK(cudaMemsetAsync(p->derr, 0, 4, p->stream));
     if (n) {
-        seen_insert_existing<<<grid_for(n), kThreads, 0, p->stream>>>(r.seen, want - 1, r.keys, n, p->derr);
+        seen_insert_existing<<<grid_for(n), kThreads, 0, p->stream>>>(r.seen, want, r.keys, n, p->derr);
         LAUNCHED();
     }
     r.seen_n = n;   // upper bound (duplicate keys of loaded rows count once in the table)
@@ -769,7 +774,7 @@ void iterate(ra_program* p, Scc& s)
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         cudaEventRecord(a, p->stream);
-        dedup_insert<<<grid_for(c[r]), kThreads, 0, p->stream>>>(out.seen, out.seen_cap - 1, p->cand + base[r], c[r],
+        dedup_insert<<<grid_for(c[r]), kThreads, 0, p->stream>>>(out.seen, out.seen_cap, p->cand + base[r], c[r],
                                                                   tag0 + base[r], p->derr);
         LAUNCHED();
         cudaEventRecord(b, p->stream);
@@ -780,7 +785,7 @@ void iterate(ra_program* p, Scc& s)
     for (size_t r = 0; r < R; r++) {
         if (!c[r]) continue;
         Relation& out = p->rels[s.rules[r].out];
-        dedup_flag<<<grid_for(c[r]), kThreads, 0, p->stream>>>(out.seen, out.seen_cap - 1, p->cand + base[r], c[r],
+        dedup_flag<<<grid_for(c[r]), kThreads, 0, p->stream>>>(out.seen, out.seen_cap, p->cand + base[r], c[r],
                                                                 tag0 + base[r], p->flag + base[r]);
         LAUNCHED();
     }
@@ -855,7 +860,7 @@ struct DevScc {
 
 size_t ctl_header_bytes() { return offsetof(IterCtl, sort_hist); }
 
-int grid_persistent() { return kSms * 4; }
+int grid_blocks(uint32_t per_sm) { return kSms * (int)per_sm; }
 
 // Can SCC s run without host work between iterations?  Every rule must read
 // rows that either are the DELTA of one of the SCC's relations (tracked on the
@@ -1032,7 +1037,7 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     for (int sl = 0; sl < pl.n_rels; sl++) {
         Relation& r = p->rels[d.rel_of_slot[sl]];
         pl.log_cap[sl] = r.cap;
-        pl.seen_limit[sl] = r.seen ? (u64)(0.65 * (double)r.seen_cap) : 0;
+        pl.seen_limit[sl] = r.seen ? (u64)(p->tune.seen_load_max * (double)r.seen_cap) : 0;
     }
 }
 
@@ -1074,7 +1079,8 @@ struct PhaseTimer {
 int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, int use_cond)
 {
     const SccPlan& pl = d.plan;
-    const int G = grid_persistent();
+    const int G = grid_blocks(p->tune.join_blocks_per_sm);
+    const int GS = grid_blocks(p->tune.select_blocks_per_sm);
     const bool ref = p->id_order == RA_IDS_REFERENCE;
     int launches = 0;
     int slot = 0;
@@ -1085,10 +1091,10 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         if (r.kind == kJoin)
             join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
                                                              p->bits, p->dcand, p->dcand_cap, out.seen,
-                                                             out.seen_cap - 1, p->dloser, p->status, slot++);
+                                                             out.seen_cap, p->dloser, p->status, slot++);
         else
             copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
-                                                                 p->dcand, p->dcand_cap, out.seen, out.seen_cap - 1,
+                                                                 p->dcand, p->dcand_cap, out.seen, out.seen_cap,
                                                                  p->dloser);
         launches++;
     }
@@ -1111,7 +1117,7 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
             a.inst_new = p->dinst_new;
             a.inst_iter_cap = p->inst_rows_cap;
         }
-        select_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, p->dloser, p->status, slot++,
+        select_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, p->dloser, p->status, slot++,
                                                      p->dhist, cond, use_cond);
         launches++;
     }
@@ -1134,7 +1140,7 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
                 a.n_rules_in = d.rm.n_rules_in[sl];
                 for (int q = 0; q < a.n_rules_in; q++) a.rules_in[q] = d.rm.rules_in[sl][q];
                 PhaseTimer pt(p, 4);
-                sort_pass_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, a, p->status, slot++);
+                sort_pass_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, a, p->status, slot++);
                 launches++;
             }
         }
@@ -1178,6 +1184,7 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
     const void* inst[2] = {p->dinst_base, p->dinst_new};
     put(inst, sizeof inst);
     put(&p->n_inst, sizeof p->n_inst);
+    put(&p->tune, sizeof p->tune);
     put(&p->inst_rows_cap, sizeof p->inst_rows_cap);
     return sig;
 }
@@ -1303,11 +1310,14 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 r.full_n = h.full_n[sl];
                 r.delta_n = h.delta_n[sl];
                 const u64 stored = r.full_n + r.delta_n;
-                if (replay && stored + incoming[sl] > r.cap) ensure_log(p, r, 2 * (stored + incoming[sl]));
-                const bool tight = h.seen_n[sl] + 2 * incoming[sl] > (u64)(0.6 * (double)r.seen_cap);
+                if (replay && stored + incoming[sl] > r.cap) ensure_log(p, r, stored + 2 * incoming[sl]);
+                const bool tight =
+                    h.seen_n[sl] + 2 * incoming[sl] > (u64)(p->tune.seen_load_max * (double)r.seen_cap);
                 if ((h.flags & kFlagProbe) || tight) {
-                    // rebuild from the stored tuples: every key older than the next (or replayed) iteration
-                    const u64 want = std::max<u64>(4 * (stored + incoming[sl]), 2 * r.seen_cap);
+                    // rebuild from the stored tuples: every key older than the next (or replayed) iteration;
+                    // at least twice the slots (a probe overflow means long clusters)
+                    const u64 want = std::max<u64>((u64)(p->tune.seen_grow * (double)(stored + incoming[sl])),
+                                                   (u64)(2.0 * p->tune.seen_load_max * (double)r.seen_cap));
                     dev_free(p, &r.seen);
                     r.seen_cap = 0;
                     build_seen(p, r, want);
@@ -1480,6 +1490,51 @@ void reset_state(ra_program* p)
     p->executed = false;
     p->running = false;
     // p->epoch keeps counting across runs: loser marks and seen-set tags are epoch-stamped
+}
+
+// Free every device buffer a run sizes (relation logs, seen sets, indexes,
+// iteration scratch) and the captured graphs; loaded rows and the packed
+// loaded state stay, so the next run re-allocates only what it needs.
+void release_buffers(ra_program* p)
+{
+    for (Relation& r : p->rels) free_relation_state(p, r);
+    dev_free(p, &p->cand);
+    dev_free(p, &p->flag);
+    dev_free(p, &p->rank);
+    dev_free(p, &p->cnt);
+    dev_free(p, &p->off);
+    dev_free(p, &p->nkeys);
+    dev_free(p, &p->nids);
+    dev_free(p, &p->tk);
+    dev_free(p, &p->tv);
+    dev_free(p, &p->hist_buf);
+    dev_free(p, &p->hist_off);
+    p->cand_cap = p->rank_cap = p->cnt_cap = p->n_cap = p->t_cap = p->hist_cap = 0;
+    dev_free(p, &p->dcand);
+    dev_free(p, &p->dloser);
+    p->dcand_cap = 0;
+    for (int q = 0; q < kMaxSccRules; q++) {
+        dev_free(p, &p->doff[q]);
+        dev_free(p, &p->dstart[q]);
+    }
+    p->doff_cap = 0;
+    for (int sl = 0; sl < kMaxSccRels; sl++) {
+        dev_free(p, &p->stage_k[sl]);
+        dev_free(p, &p->stage_v[sl]);
+    }
+    for (int b = 0; b < 2; b++) {
+        dev_free(p, &p->sort_k[b]);
+        dev_free(p, &p->sort_v[b]);
+    }
+    p->stage_cap = 0;
+    dev_free(p, &p->status);
+    p->status_cap = 0;
+    dev_free(p, &p->dinst_new);
+    p->inst_rows_cap = 0;
+    dev_free(p, &p->dhist);
+    p->dhist_cap = 0;
+    for (Scc& sc : p->sccs) drop_graph(sc);
+    CK(cudaStreamSynchronize(p->stream));
 }
 
 void begin_run(ra_program* p)
@@ -1886,6 +1941,15 @@ int ra_program_run_next_scc(ra_program* p, int* scc_id)
     });
 }
 
+int ra_program_release(ra_program* p)
+{
+    return guard(p, [&] {
+        if (p->running) fail(p, RA_E_STATE, "release during a run");
+        release_buffers(p);
+        reset_state(p);   // the last run's results lived in the freed logs
+    });
+}
+
 int ra_program_reset(ra_program* p)
 {
     return guard(p, [&] {
@@ -1907,6 +1971,29 @@ int ra_program_iteration_times(ra_program* p, double* out_us, uint64_t cap, uint
     return guard(p, [&] {
         if (len) *len = p->iter_us.size();
         if (out_us) std::memcpy(out_us, p->iter_us.data(), std::min<u64>(cap, p->iter_us.size()) * 8);
+    });
+}
+
+int ra_program_get_tuning(ra_program* p, ra_tuning* out)
+{
+    return guard(p, [&] {
+        if (!out) fail(p, RA_E_BADARG, "null tuning");
+        *out = p->tune;
+    });
+}
+
+int ra_program_set_tuning(ra_program* p, const ra_tuning* t)
+{
+    return guard(p, [&] {
+        if (!t) fail(p, RA_E_BADARG, "null tuning");
+        if (p->running) fail(p, RA_E_STATE, "set_tuning during a run");
+        if (!(t->seen_load_max >= 0.1 && t->seen_load_max <= 0.9)) fail(p, RA_E_BADARG, "seen_load_max outside [0.1, 0.9]");
+        if (!(t->seen_grow >= 1.1 && t->seen_grow <= 8.0)) fail(p, RA_E_BADARG, "seen_grow outside [1.1, 8]");
+        if (!(t->log_growth >= 1.1 && t->log_growth <= 4.0)) fail(p, RA_E_BADARG, "log_growth outside [1.1, 4]");
+        if (t->join_blocks_per_sm < 1 || t->join_blocks_per_sm > 16 || t->select_blocks_per_sm < 1 ||
+            t->select_blocks_per_sm > 16)
+            fail(p, RA_E_BADARG, "blocks per SM outside [1, 16]");
+        p->tune = *t;
     });
 }
 

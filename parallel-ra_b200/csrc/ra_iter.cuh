@@ -246,7 +246,7 @@ struct LoserMarks {
     u64 epoch_tag;  // epoch << 40: tags below it belong to tuples from earlier iterations
 };
 
-__device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 mask, u64 k, u64 mine, u64 h, Slot cur,
+__device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 cap, u64 k, u64 mine, u64 h, Slot cur,
                                            const LoserMarks& lm, u32* flags)
 {
     const Slot empty{kEmpty, ~0ull};
@@ -268,13 +268,13 @@ __device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 mask, u64 k
                 cur = prev;
             }
         }
-        h = (h + 1) & mask;
+        h = slot_next(h, cap);
         cur = atomicCAS(&t[h], empty, mineslot);
     }
     atomicOr(flags, kFlagProbe);
 }
 
-__device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 mask, const u64* key, const u64* mine,
+__device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 cap, const u64* key, const u64* mine,
                                             const bool* valid, const LoserMarks& lm, u32* flags)
 {
     const Slot empty{kEmpty, ~0ull};
@@ -282,12 +282,12 @@ __device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 mask, cons
     u64 h[kClaimBatch];
 #pragma unroll
     for (int k = 0; k < kClaimBatch; k++) {
-        h[k] = mix64(key[k]) & mask;
+        h[k] = slot_start(key[k], cap);
         if (valid[k]) cur[k] = atomicCAS(&t[h[k]], empty, Slot{key[k], mine[k]});
     }
 #pragma unroll
     for (int k = 0; k < kClaimBatch; k++)
-        if (valid[k]) claim_rest(t, mask, key[k], mine[k], h[k], cur[k], lm, flags);
+        if (valid[k]) claim_rest(t, cap, key[k], mine[k], h[k], cur[k], lm, flags);
 }
 
 __device__ __forceinline__ LoserMarks loser_marks(const IterCtl* c, u32* mark)
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                                                               int outer_shift, const u64* __restrict__ csr,
                                                               const u64* __restrict__ inner, Projection pj, int bits,
                                                               u64* __restrict__ cand, u64 cand_cap,
-                                                              Slot* __restrict__ seen, u64 seen_mask,
+                                                              Slot* __restrict__ seen, u64 seen_cap,
                                                               u32* __restrict__ loser, u64* __restrict__ status,
                                                               int tile_slot)
 {
@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                     mine[k] = tag_base + prefix + j;
                     if (valid[k]) cand[cbase + prefix + j] = key[k];
                 }
-                claim_batch(seen, seen_mask, key, mine, valid, lm, &ctl->flags);
+                claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
             }
         }
         __syncthreads();
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
 __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restrict__ ctl, SccPlan plan, int rule,
                                                               RowsRef in_ref, Projection pj, int bits, int pred,
                                                               u64* __restrict__ cand, u64 cand_cap,
-                                                              Slot* __restrict__ seen, u64 seen_mask,
+                                                              Slot* __restrict__ seen, u64 seen_cap,
                                                               u32* __restrict__ loser)
 {
     if (ctl->flags) return;
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
                 valid[k] = keep;
             }
         }
-        claim_batch(seen, seen_mask, key, mine, valid, lm, &ctl->flags);
+        claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
     }
     (void)plan;
 }

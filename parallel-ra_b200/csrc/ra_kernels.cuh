@@ -197,11 +197,18 @@ struct alignas(16) Slot {
 };
 __device__ __forceinline__ bool slot_eq(const Slot& a, const Slot& b) { return a.key == b.key && a.tag == b.tag; }
 
+// A seen set has `cap` slots, any count: a key's probe run starts at
+// floor(mix64(k) * cap / 2^64) (multiplicative range reduction, so the table
+// needs no power-of-two size and its load factor is exactly what the host
+// sized it for) and steps linearly, wrapping at cap.
+__device__ __forceinline__ u64 slot_start(u64 k, u64 cap) { return __umul64hi(mix64(k), cap); }
+__device__ __forceinline__ u64 slot_next(u64 h, u64 cap) { return h + 1 == cap ? 0 : h + 1; }
+
 // Returns the slot holding k (inserting it if absent), or ~0 if the table is full.
-__device__ __forceinline__ u64 seen_find_or_insert(Slot* __restrict__ t, u64 mask, u64 k)
+__device__ __forceinline__ u64 seen_find_or_insert(Slot* __restrict__ t, u64 cap, u64 k)
 {
-    u64 h = mix64(k) & mask;
-    for (u64 probe = 0; probe <= mask; probe++) {
+    u64 h = slot_start(k, cap);
+    for (u64 probe = 0; probe < cap; probe++) {
         u64 cur = *((volatile u64*)&t[h].key);
         if (cur == k) return h;
         if (cur == kEmpty) {
@@ -209,43 +216,43 @@ __device__ __forceinline__ u64 seen_find_or_insert(Slot* __restrict__ t, u64 mas
             if (prev == kEmpty || prev == k) return h;
             continue;   // lost the slot to another key: re-examine nothing, move on
         }
-        h = (h + 1) & mask;
+        h = slot_next(h, cap);
     }
     return ~0ull;
 }
 
-__device__ __forceinline__ u64 seen_find(const Slot* __restrict__ t, u64 mask, u64 k)
+__device__ __forceinline__ u64 seen_find(const Slot* __restrict__ t, u64 cap, u64 k)
 {
-    u64 h = mix64(k) & mask;
-    for (u64 probe = 0; probe <= mask; probe++) {
+    u64 h = slot_start(k, cap);
+    for (u64 probe = 0; probe < cap; probe++) {
         u64 cur = t[h].key;
         if (cur == k) return h;
         if (cur == kEmpty) return ~0ull;
-        h = (h + 1) & mask;
+        h = slot_next(h, cap);
     }
     return ~0ull;
 }
 
 // Insert existing tuples with tag 0 (seen before any running iteration).
-__global__ void __launch_bounds__(kThreads) seen_insert_existing(Slot* __restrict__ t, u64 mask,
+__global__ void __launch_bounds__(kThreads) seen_insert_existing(Slot* __restrict__ t, u64 cap,
                                                                  const u64* __restrict__ keys, u64 n,
                                                                  u32* __restrict__ err)
 {
     for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads) {
-        u64 h = seen_find_or_insert(t, mask, keys[i]);
+        u64 h = seen_find_or_insert(t, cap, keys[i]);
         if (h == ~0ull) { *err = 1u; continue; }
         atomicMin(&t[h].tag, 0ull);
     }
 }
 
 // Candidate p (global stream position base + i) claims the first occurrence of its key.
-__global__ void __launch_bounds__(kThreads) dedup_insert(Slot* __restrict__ t, u64 mask, const u64* __restrict__ cand,
+__global__ void __launch_bounds__(kThreads) dedup_insert(Slot* __restrict__ t, u64 cap, const u64* __restrict__ cand,
                                                          u64 n, u64 tag_base, u32* __restrict__ err)
 {
     for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads) {
         const u64 k = cand[i];
         if (k == kEmpty) continue;
-        u64 h = seen_find_or_insert(t, mask, k);
+        u64 h = seen_find_or_insert(t, cap, k);
         if (h == ~0ull) { *err = 1u; continue; }
         const u64 mine = tag_base + i;
         if (t[h].tag > mine) atomicMin(&t[h].tag, mine);
@@ -253,14 +260,14 @@ __global__ void __launch_bounds__(kThreads) dedup_insert(Slot* __restrict__ t, u
 }
 
 // flag[i] = 1 when candidate i is the first occurrence of a tuple new to the relation.
-__global__ void __launch_bounds__(kThreads) dedup_flag(const Slot* __restrict__ t, u64 mask, const u64* __restrict__ cand,
+__global__ void __launch_bounds__(kThreads) dedup_flag(const Slot* __restrict__ t, u64 cap, const u64* __restrict__ cand,
                                                        u64 n, u64 tag_base, u32* __restrict__ flag)
 {
     for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads) {
         const u64 k = cand[i];
         u32 f = 0;
         if (k != kEmpty) {
-            u64 h = seen_find(t, mask, k);
+            u64 h = seen_find(t, cap, k);
             f = (h != ~0ull && t[h].tag == tag_base + i) ? 1u : 0u;
         }
         flag[i] = f;

@@ -16,6 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # RA_ENGINE_LIB: path of another build of the engine library (e.g. a tuning variant)
 LIB_PATH = os.environ.get("RA_ENGINE_LIB") or os.path.join(HERE, "libra_b200.so")
 
+# autotuner output (autotune.py); RA_TUNING_FILE names another file, or "none"
+TUNING_PATH = os.path.join(HERE, "tuning.json")
+
 DELTA, FULL = 0, 1
 COPY, ACOPY, COPY_FILTER = 0, 1, 2
 IDS_EMISSION, IDS_REFERENCE = 0, 1
@@ -29,6 +32,7 @@ EXPORTS = (
     "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats", "ra_program_iteration_times",
     "ra_relation_counts", "ra_relation_dump_full", "ra_rows_distinct_noalloc", "ra_status_string", "ra_last_error",
     "ra_program_set_instances", "ra_program_instance_history", "ra_relation_instance_summary",
+    "ra_program_get_tuning", "ra_program_set_tuning", "ra_program_release",
 )
 
 
@@ -48,6 +52,18 @@ class Stats(C.Structure):
         ("device_bytes_peak", C.c_uint64),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
+
+
+class Tuning(C.Structure):
+    """ra_tuning: hash load factor, growth factors and kernel grid shapes of a program."""
+    _fields_ = [
+        ("seen_load_max", C.c_double), ("seen_grow", C.c_double), ("log_growth", C.c_double),
+        ("join_blocks_per_sm", C.c_uint32), ("select_blocks_per_sm", C.c_uint32),
+    ]
+    FIELDS = ("seen_load_max", "seen_grow", "log_growth", "join_blocks_per_sm", "select_blocks_per_sm")
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in self.FIELDS}
 
 
 _lib = None
@@ -81,12 +97,15 @@ def lib():
         L.ra_program_execute.argtypes = [P]
         L.ra_program_run_next_scc.argtypes = [P, i32p]
         L.ra_program_reset.argtypes = [P]
+        L.ra_program_release.argtypes = [P]
         L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
         L.ra_program_iteration_times.argtypes = [P, C.POINTER(C.c_double), C.c_uint64, u64p]
         L.ra_relation_counts.argtypes = [P, C.c_int, u64p, u64p]
         L.ra_relation_dump_full.argtypes = [P, C.c_int, u64p, C.c_uint64, u64p]
         L.ra_program_set_instances.argtypes = [P, u64p, C.c_uint32]
+        L.ra_program_get_tuning.argtypes = [P, C.POINTER(Tuning)]
+        L.ra_program_set_tuning.argtypes = [P, C.POINTER(Tuning)]
         L.ra_program_instance_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_relation_instance_summary.argtypes = [P, C.c_int, u64p, u64p]
         L.ra_rows_distinct_noalloc.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -96,6 +115,16 @@ def lib():
         L.ra_last_error.restype = C.c_char_p
         _lib = L
     return _lib
+
+
+def tuning_file() -> dict | None:
+    """The autotuner's saved result, if any (see autotune.py)."""
+    path = os.environ.get("RA_TUNING_FILE") or TUNING_PATH
+    if path == "none" or not os.path.exists(path):
+        return None
+    import json
+    with open(path) as f:
+        return json.load(f)
 
 
 def _u64(a: np.ndarray):
@@ -114,6 +143,9 @@ class Program:
         self._p = h
         self._arity = {}
         self._n_inst = 0
+        tuned = tuning_file()
+        if tuned:
+            self.set_tuning(**tuned["tuning"])
         if id_order is not None:
             self.set_id_order(id_order)
 
@@ -189,6 +221,10 @@ class Program:
             self.set_batch_size(batch_size)
         self._ck(self._L.ra_program_execute(self._p), "execute")
 
+    def release(self):
+        """Free the device buffers kept between runs (ends the last run)."""
+        self._ck(self._L.ra_program_release(self._p), "release")
+
     def reset(self):
         self._ck(self._L.ra_program_reset(self._p), "reset")
 
@@ -259,3 +295,18 @@ class Program:
         self._ck(self._L.ra_relation_instance_summary(self._p, rel, _u64(counts), _u64(digests)),
                  "instance_summary")
         return counts, digests
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        self._ck(self._L.ra_program_get_tuning(self._p, C.byref(t)), "get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Change some tuning fields (see ra_tuning in include/ra_engine.h); others keep their values."""
+        t = Tuning()
+        self._ck(self._L.ra_program_get_tuning(self._p, C.byref(t)), "get_tuning")
+        for k, v in kw.items():
+            if k not in Tuning.FIELDS:
+                raise KeyError(k)
+            setattr(t, k, v)
+        self._ck(self._L.ra_program_set_tuning(self._p, C.byref(t)), "set_tuning")
