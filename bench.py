@@ -324,10 +324,15 @@ BATCH_SERIAL_SAMPLE = 512
 BATCH_CPU_SAMPLE = 12
 
 
+def gen_processes():
+    return max(1, min(32, (os.cpu_count() or 2) - 1))
+
+
 def batched_instances(count, seed):
     """The batched workload: per-instance seeded ER graphs (datagen.batched_sizes)."""
     import parallel_ra_b200 as P
-    return [P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, s)) for n, m, s in P.datagen.batched_sizes(count, seed)]
+    return P.datagen.generate_many([("er", n, m, s) for n, m, s in P.datagen.batched_sizes(count, seed)],
+                                   gen_processes())
 
 
 def batched_cpu_baseline(insts, total_tuples):
@@ -484,13 +489,107 @@ def run_batched(args, rank, world, local_rank):
     return line
 
 
+SERVED_COUNT, SERVED_SEED = 20000, 4
+SERVED_RATES = (100.0, 1000.0, 10000.0)
+SERVED_POINT_SECONDS = 10.0
+SERVED_CHECK_SAMPLE = 400
+
+
+def run_served(args, rank, world, local_rank):
+    """Open-loop Poisson request streams (80% TC, 20% SG, 2% large TC) against the
+    continuous-batching server, swept over arrival rates; latency percentiles and
+    instances/s per rate, every checked result equal to a plain single-instance run."""
+    import torch
+    import parallel_ra_b200 as P
+    from parallel_ra_b200.serve import Request, Server, poisson_arrivals, request_mix, run_stream
+
+    torch.cuda.set_device(local_rank)
+    reqs = request_mix(SERVED_COUNT, SERVED_SEED + 1000 * rank, processes=gen_processes())
+    from parallel_ra_b200.batch import estimate_tuples
+    for r in reqs:
+        r.est_tuples = estimate_tuples(r.kind, r.rows)
+
+    def clones(sub):
+        return [Request(r.rid, r.kind, r.rows, est_tuples=r.est_tuples) for r in sub]
+
+    server = Server(local_rank, slots=args.slots, budget_bytes=args.budget_gb * 1e9)
+    for _ in range(args.warmup):               # warm-up streams: graphs, buffers, learnt estimates
+        run_stream(server, clones(reqs[:500]), poisson_arrivals(500, max(SERVED_RATES), 99))
+    points = []
+    top = None
+    with ClockSampler(local_rank) as clocks:
+        for rate in SERVED_RATES:
+            k = SERVED_COUNT if rate == max(SERVED_RATES) else min(SERVED_COUNT, int(rate * SERVED_POINT_SECONDS))
+            stream = clones(reqs[:k])
+            w0 = len(server.waves)
+            st = run_stream(server, stream, poisson_arrivals(k, rate, 7))
+            waves = server.waves[w0:]
+            st["rate"] = rate
+            st["waves"] = len(waves)
+            st["mean_wave_size"] = float(np.mean([w.size for w in waves]))
+            st["gpu_launches"] = int(sum(w.launches for w in waves))
+            st["max_held_gb"] = max(w.held_bytes for w in waves) / 1e9
+            points.append(st)
+            if rate == max(SERVED_RATES):
+                top = (stream, st)
+    server.close()
+
+    # every sampled result of the top-rate stream equals its plain single-instance run
+    stream, st_top = top
+    rng = np.random.default_rng(11)
+    sample = rng.choice(len(stream), min(SERVED_CHECK_SAMPLE, len(stream)), replace=False)
+    plain = {"tc": P.batch.Runner("tc", local_rank), "sg": P.batch.Runner("sg", local_rank)}
+    mismatches = sum(int(stream[int(i)].result is None or stream[int(i)].result.key() != plain[
+        stream[int(i)].kind].run_plain(stream[int(i)].rows).key()) for i in sample)
+    for r in plain.values():
+        r.close()
+    if mismatches:
+        raise RuntimeError(f"{mismatches} served results differ from their plain runs")
+
+    # the same stream served one instance at a time (no batching, one worker)
+    one = Server(local_rank, slots=1, budget_bytes=args.budget_gb * 1e9, max_wave_requests=1)
+    k1 = 1500
+    st_one = run_stream(one, clones(reqs[:k1]), poisson_arrivals(k1, max(SERVED_RATES), 7))
+    one.close()
+    if rank != 0:
+        return None
+    h2d = int(sum(r.rows.nbytes for r in stream))
+    line = {
+        "metric": "served instances/s", "value": st_top["instances_per_s"], "unit": "instances/s",
+        "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": 1e3 * st_top["seconds"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "served", "requests": SERVED_COUNT, "seed": SERVED_SEED,
+                   "mix": "80% TC (ER, n log-uniform [64, 16384], degree U[0.8, 2.0]), 20% SG (random trees, "
+                          "n log-uniform [64, 16384]), 2% of all requests large TC (ER n=2^18, degree 0.95)",
+                   "slots": args.slots, "budget_gb": args.budget_gb, "rates": points,
+                   "p50_ms": st_top["p50_ms"], "p95_ms": st_top["p95_ms"], "p99_ms": st_top["p99_ms"],
+                   "timing": "host wall clock from each request's submission to its results on the host; "
+                             "step = the whole top-rate stream",
+                   "metric_family": METRIC_FAMILY},
+        "one_at_a_time": {"value": st_one["instances_per_s"], "unit": "instances/s", "requests": k1,
+                          "p50_ms": st_one["p50_ms"], "p99_ms": st_one["p99_ms"],
+                          "mode": "same server, one worker, waves of one request (plain runs)"},
+        "admission": {"oom_retries": int(server.oom_retries), "unserved": int(sum(r.error is not None for r in stream)),
+                      "learnt_bytes_per_tuple": server.bpt, "learnt_size_correction": server.correction},
+        "bit_exact": {"checked": int(len(sample)), "mismatches": mismatches,
+                      "against": "plain single-instance runs of the same requests"},
+        "clocks": clocks.summary(),
+        "e2e": {"value": st_top["instances_per_s"], "unit": "instances/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(8 * 4 * len(stream))},
+        "gpu_launches": int(st_top["gpu_launches"]),
+    }
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tc-er22", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--workload", default="tc-er22", choices=sorted(WORKLOADS) + ["batched", "served"])
+    ap.add_argument("--slots", type=int, default=4, help="served: concurrent waves (worker threads)")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="served: device-memory admission budget")
     ap.add_argument("--wave-tuples", type=float, default=0.0,
                     help="batched: estimated derived tuples per wave (default: the autotuned size, "
                          "capped by half the free device memory)")
@@ -512,6 +611,8 @@ def main():
         line = run_reference_arm(args, rank, world)
     elif args.workload == "batched":
         line = run_batched(args, rank, world, local_rank)
+    elif args.workload == "served":
+        line = run_served(args, rank, world, local_rank)
     else:
         line = run_ours(args, rank, world, local_rank)
         if world > 1:

@@ -1927,18 +1927,39 @@ int ra_scc_depend(ra_program* p, int src_scc, int dst_scc)
     });
 }
 
+// A run that failed (out of device memory, a device wait that timed out, ...)
+// leaves the program reusable: an open stream capture is closed, queued work
+// drains, and the run ends -- the next execute starts from the loaded state
+// and ra_program_release can free what the failed run had allocated.
+static int end_failed_run(ra_program* p, int st)
+{
+    if (st == RA_OK || !p) return st;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (p->stream && cudaStreamIsCapturing(p->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(p->stream, &g);
+        if (g) cudaGraphDestroy(g);
+    }
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    cudaGetLastError();   // clear a non-sticky error (allocation failure) left by the run
+    for (Scc& sc : p->sccs) drop_graph(sc);
+    p->running = false;
+    p->executed = false;
+    return st;
+}
+
 int ra_program_execute(ra_program* p)
 {
-    return guard(p, [&] { execute(p); });
+    return end_failed_run(p, guard(p, [&] { execute(p); }));
 }
 
 int ra_program_run_next_scc(ra_program* p, int* scc_id)
 {
-    return guard(p, [&] {
+    return end_failed_run(p, guard(p, [&] {
         int id = -1;
         if (!(p->executed && !p->running)) id = step(p);
         if (scc_id) *scc_id = id;
-    });
+    }));
 }
 
 int ra_program_release(ra_program* p)

@@ -22,6 +22,8 @@ TUNING_PATH = os.path.join(HERE, "tuning.json")
 DELTA, FULL = 0, 1
 COPY, ACOPY, COPY_FILTER = 0, 1, 2
 IDS_EMISSION, IDS_REFERENCE = 0, 1
+# status codes of include/ra_engine.h
+E_BADARG, E_IO, E_OOM, E_CUDA, E_UNSUPPORTED, E_TIMEOUT, E_STATE = 1, 2, 3, 4, 5, 6, 7
 
 # every entry point declared in include/ra_engine.h
 EXPORTS = (
