@@ -40,13 +40,16 @@ sys.path.insert(0, ROOT)
 METRIC = "TC tuples/s"
 METRIC_FAMILY = "TC tuples/s + HBM GB/s on 1 B200; batched vs serial instances/s; p99 ms"
 WORKLOADS = {
-    # name: (nodes, edges, seed)
-    "tc-er22": (1 << 22, 3984589, 2),
-    "tc-er20": (1 << 20, 996147, 2),        # same family at 1/4 scale (profiling case)
-    "tc-er2000": (2000, 3000, 1),
+    # name: (program, graph generator, generator arguments)
+    "tc-er22": ("tc", "er", (1 << 22, 3984589, 2)),
+    "tc-er20": ("tc", "er", (1 << 20, 996147, 2)),    # same family at 1/4 scale (profiling case)
+    "tc-er2000": ("tc", "er", (2000, 3000, 1)),
+    "sg-tree15": ("sg", "tree", (1 << 15, 3)),         # same generation on a random tree of 2^15 nodes
 }
-# bounded CPU sample of the same graph family (mean out-degree 0.95)
-CPU_SAMPLE = (1 << 17, round(0.95 * (1 << 17)), 2)
+OUTPUT = {"tc": "T", "sg": "SG"}
+INPUT = {"tc": "G", "sg": "edge"}
+# bounded CPU samples of the same graph families
+CPU_SAMPLES = {"tc": ("er", (1 << 17, round(0.95 * (1 << 17)), 2)), "sg": ("tree", (1 << 12, 3))}
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
 # ncu capture in profiles/join_fused_kernel_tc-er20.md (1.79 / 1.81 / 1.83 over
@@ -119,14 +122,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def reference_sample_run(n, m, seed):
-    """Run the reference (oracle/_ref/ref_driver) once; returns (tc_tuples, seconds, kind)."""
+def workload_rows(gen, params):
     import parallel_ra_b200 as P
-    return reference_rows_run(P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, seed)))
+    if gen == "er":
+        return P.datagen.with_row_ids(P.datagen.erdos_renyi(*params))
+    return P.datagen.with_row_ids(P.datagen.random_tree(*params))
 
 
-def reference_rows_run(rows):
-    """TC of ``rows`` by the reference's CPU code; returns (tc_tuples, fixpoint seconds, kind)."""
+def reference_sample_run(kind):
+    """The reference's CPU code on the bounded sample of a program's graph family."""
+    gen, params = CPU_SAMPLES[kind]
+    return reference_rows_run(workload_rows(gen, params), kind)
+
+
+def reference_rows_run(rows, kind="tc"):
+    """Program ``kind`` on ``rows`` by the reference's CPU code; returns (output tuples, fixpoint seconds, kind)."""
     import parallel_ra_b200 as P
     drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
     if os.path.exists(drv):
@@ -134,21 +144,31 @@ def reference_rows_run(rows):
             edge, empty, out = (os.path.join(tmp, x) for x in ("edge", "empty", "out"))
             P.datagen.write_relation(edge, rows)
             P.datagen.write_empty_relation(empty)
-            subprocess.run([drv, "tc", edge, empty, out], check=True, stdout=subprocess.DEVNULL)
+            subprocess.run([drv, kind, edge, empty, out], check=True, stdout=subprocess.DEVNULL)
             secs = float(open(os.path.join(out, "time.txt")).read())
-            tc = next(int(l.split()[2]) for l in open(os.path.join(out, "sizes.txt")) if l.split()[0] == "T")
+            tc = next(int(l.split()[2]) for l in open(os.path.join(out, "sizes.txt"))
+                      if l.split()[0] == OUTPUT[kind])
         return tc, secs, "reference"
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     p = O.OracleProgram()
-    rels = P.programs.build_tc(p, rows)
+    rels = P.programs.PROGRAMS[kind](p, rows)
     p.execute(1)
-    return p.full_count(rels["T"]), p.fixpoint_seconds(), "port"
+    return p.full_count(rels[OUTPUT[kind]]), p.fixpoint_seconds(), "port"
 
 
-def cpu_sample_desc():
-    n, m, s = CPU_SAMPLE
-    return f"TC on ER n={n} m={m} seed={s} (same family as the workload, mean out-degree 0.95), fixpoint time only"
+def cpu_sample_desc(kind="tc"):
+    gen, params = CPU_SAMPLES[kind]
+    if gen == "er":
+        n, m, s = params
+        return (f"TC on ER n={n} m={m} seed={s} (same family as the workload, mean out-degree 0.95), "
+                f"fixpoint time only")
+    n, s = params
+    return f"SG on a random tree of n={n} nodes seed={s} (same family as the workload), fixpoint time only"
+
+
+def metric_of(kind):
+    return f"{OUTPUT[kind]} tuples/s" if kind == "sg" else METRIC
 
 
 def run_reference_arm(args, rank, world):
@@ -168,21 +188,22 @@ def run_reference_arm(args, rank, world):
                                                 "metric_family": METRIC_FAMILY},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "instances/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
-    n, m, s = CPU_SAMPLE
+    prog_kind = WORKLOADS[args.workload][0]
     vals = []
     for i in range(args.warmup + args.steps):
-        tc, secs, kind = reference_sample_run(n, m, s)
+        tc, secs, kind = reference_sample_run(prog_kind)
         if i >= args.warmup:
             vals.append((tc, secs))
     tot_tc = sum(v[0] for v in vals)
     tot_s = sum(v[1] for v in vals)
     value = tot_tc / tot_s
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_of(prog_kind), "value": value, "unit": "tuples/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / len(vals), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": cpu_sample_desc(), "metric_family": METRIC_FAMILY},
-        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": 1, "kind": kind, "sample": cpu_sample_desc()},
+        "config": {"workload": args.workload, "sample": cpu_sample_desc(prog_kind), "metric_family": METRIC_FAMILY},
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": 1, "kind": kind,
+                         "sample": cpu_sample_desc(prog_kind)},
         "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -193,18 +214,19 @@ def run_ours(args, rank, world, local_rank):
     import parallel_ra_b200 as P
 
     torch.cuda.set_device(local_rank)
-    n, m, seed = WORKLOADS[args.workload]
-    seed = seed + 1000 * rank          # each rank: its own independent instance
-    rows = P.datagen.with_row_ids(P.datagen.erdos_renyi(n, m, seed))
+    prog_kind, gen, params = WORKLOADS[args.workload]
+    params = params[:-1] + (params[-1] + 1000 * rank,)     # each rank: its own independent instance
+    rows = workload_rows(gen, params)
     stream = torch.cuda.Stream()
     prog = P.Program(local_rank)
     prog.set_stream(stream.cuda_stream)
-    rels = P.programs.build_tc(prog, rows)
+    rels = P.programs.PROGRAMS[prog_kind](prog, rows)
+    out_rel, in_rel = rels[OUTPUT[prog_kind]], rels[INPUT[prog_kind]]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f"cuda:{local_rank}")
 
     for _ in range(args.warmup):
         prog.execute(1)
-    tc = prog.full_count(rels["T"])
+    tc = prog.full_count(out_rel)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -273,12 +295,13 @@ def run_ours(args, rank, world, local_rank):
     for i in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        prog.load_rows(rels["G"], pinned_np)
-        prog.load_rows(rels["T"], np.empty((0, 3), dtype=np.uint64))
+        prog.load_rows(in_rel, pinned_np)
+        for name, h_rel in rels.items():
+            if h_rel != in_rel:
+                prog.load_rows(h_rel, np.empty((0, 3), dtype=np.uint64))
         prog.execute(1)
         h = prog.history()
-        f, _ = prog.counts(rels["T"])
-        g, _ = prog.counts(rels["G"])
+        f, _ = prog.counts(out_rel)
         e2e_s.append(time.perf_counter() - t0)
         d2h = 8 * (2 + sum(2 + 2 * len(x[1]) for x in h))
         assert f == tc
@@ -298,11 +321,12 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return None
     line = {
-        "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_of(prog_kind), "value": value, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": args.workload, "nodes": n, "edges": m, "seed": WORKLOADS[args.workload][2],
-                   "tc_tuples": tc, "iterations": int(st.iterations), "join_candidates": int(st.join_candidates),
+        "config": {"workload": args.workload, "program": prog_kind, "generator": gen, "generator_args": list(params),
+                   "input_rows": int(rows.shape[0]), "output_tuples": tc, "iterations": int(st.iterations),
+                   "join_candidates": int(st.join_candidates),
                    "value_bits": int(st.value_bits), "l2": "flushed (256 MiB write) before every timed step",
                    "id_order": "emission (default)",
                    "value_reference_ids": tc / (statistics.median(ref_ms) / 1e3),
@@ -313,9 +337,9 @@ def run_ours(args, rank, world, local_rank):
         "step_ms": step_ms,
     }
     if world == 1 and not args.no_cpu_baseline:
-        ctc, csecs, kind = reference_sample_run(*CPU_SAMPLE)
+        ctc, csecs, kind = reference_sample_run(prog_kind)
         line["cpu_baseline"] = {"value": ctc / csecs, "unit": "tuples/s", "cores": 1, "kind": kind,
-                                "sample": cpu_sample_desc()}
+                                "sample": cpu_sample_desc(prog_kind)}
     return line
 
 
