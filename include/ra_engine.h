@@ -97,6 +97,7 @@ typedef struct ra_stats {
     uint64_t regrows;           /* buffer regrowths (iteration retried) */
     uint64_t device_bytes;      /* device memory the program holds after the run */
     uint64_t device_bytes_peak; /* most device memory it held during the run */
+    uint64_t dense_sccs;        /* SCCs run by the dense row-closure evaluator */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose
@@ -109,13 +110,21 @@ typedef struct ra_stats {
  *                       stored and arriving (1.1 .. 8): fewer rebuilds vs memory
  *   log_growth          capacity factor when a relation's tuple log grows (1.1 .. 4)
  *   join_blocks_per_sm  CTAs per SM of the fused join kernel (1 .. 16)
- *   select_blocks_per_sm  CTAs per SM of the winner-selection kernel (1 .. 16) */
+ *   select_blocks_per_sm  CTAs per SM of the winner-selection kernel (1 .. 16)
+ *   dense_max_bytes     device bytes the dense row-closure evaluator may use for
+ *                       its bit matrices (0 switches it off).  A fixed-point SCC
+ *                       whose one rule has the transitive-closure shape
+ *                       R(z,x) :- R_delta(y,x), S_full(y,z) over values (per
+ *                       instance) below 65,536 runs as one breadth-first search
+ *                       per row of R in shared memory instead of the hash-set
+ *                       path (emission id order, batch size 1). */
 typedef struct ra_tuning {
     double seen_load_max;
     double seen_grow;
     double log_growth;
     uint32_t join_blocks_per_sm;
     uint32_t select_blocks_per_sm;
+    double dense_max_bytes;
 } ra_tuning;
 
 /* Create a program on CUDA device `device`.  Replaces the per-rank set-up of

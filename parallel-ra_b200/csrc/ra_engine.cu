@@ -16,7 +16,7 @@
 //   * RAM::check_for_fixed_point's MPI_Allreduce (RA_tasks.cpp:1072-1085):
 //     device counters.
 #include "../../include/ra_engine.h"
-#include "ra_iter.cuh"
+#include "ra_dense.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -124,7 +124,7 @@ struct ra_program {
     bool own_stream = false;
     uint32_t batch_size = 1;
     int id_order = RA_IDS_EMISSION;
-    ra_tuning tune = {0.45, 4.0, 1.5, 4, 4};   // the autotuner's B200 choice (tuning.json)
+    ra_tuning tune = {0.45, 4.0, 1.5, 4, 4, 8e9};   // the autotuner's B200 choice (tuning.json)
     std::vector<Relation> rels;
     std::vector<Scc> sccs;
     std::vector<std::pair<int, int>> deps;
@@ -132,6 +132,7 @@ struct ra_program {
     std::vector<double> iter_us;  // device time of each device-driven iteration of the last run
     std::vector<std::pair<uint32_t, u64>> intern;   // (tag, next counter) -- LIE::intern_map
     int bits = 0;                 // packed bits per column for this run
+    u64 max_value = 0;            // largest data value loaded (sets `bits`)
     bool packed = false;          // loaded relations packed with `bits` (cleared by a new load)
     bool executed = false;
     bool running = false;         // between the first and the last SCC of a run
@@ -1395,6 +1396,205 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     p->history.insert(p->history.end(), hist.begin(), hist.end());
 }
 
+// Device buffers of one dense evaluation, freed on every exit.
+struct DenseBufs {
+    ra_program* p;
+    u32* known = nullptr;
+    u32* delta0 = nullptr;
+    u64* row_new = nullptr;
+    u64* row_off = nullptr;
+    u64* level_total = nullptr;
+    u64* counters = nullptr;
+    u32* flags = nullptr;
+    DenseInst* inst = nullptr;
+    explicit DenseBufs(ra_program* pp) : p(pp) {}
+    ~DenseBufs()
+    {
+        dev_free(p, &known);
+        dev_free(p, &delta0);
+        dev_free(p, &row_new);
+        dev_free(p, &row_off);
+        dev_free(p, &level_total);
+        dev_free(p, &counters);
+        dev_free(p, &flags);
+        dev_free(p, &inst);
+    }
+};
+
+// Runs SCC s with the dense row-closure evaluator (ra_dense.cuh) when its one
+// rule has the transitive-closure shape and the bit matrices fit the tuned
+// budget; returns false (nothing done) otherwise.  Leaves the SCC's relations
+// as the semi-naive loop would after its fixed point (new tuples appended to
+// R's log, everything in R's full version after the caller's delta_to_full),
+// and records the same per-iteration history (RAM::check_for_fixed_point,
+// src/RAM/RA_tasks.cpp:1072-1085) and per-instance counts.
+bool run_scc_dense(ra_program* p, Scc& s)
+{
+    if (!s.fixpoint || s.rules.size() != 1 || s.rules[0].kind != kJoin) return false;
+    if (p->id_order != RA_IDS_EMISSION || p->batch_size != 1 || p->tune.dense_max_bytes <= 0) return false;
+    const Rule& ru = s.rules[0];
+    const JoinPlan jp = make_join_plan(p, ru);
+    if (jp.outer_rel != ru.out || jp.outer_ver != RA_DELTA || jp.inner_ver != RA_FULL || jp.inner_rel == ru.out)
+        return false;
+    Relation& R = p->rels[ru.out];
+    Relation& S = p->rels[jp.inner_rel];
+    if (R.arity != 2 || S.arity != 2 || R.jcc != 1) return false;
+    const Projection& pj = jp.pj;
+    if (pj.n != 2 || pj.side[0] != 1 || pj.col[0] != 1 || pj.side[1] != 0 || pj.col[1] != 1) return false;
+    if (std::find(s.rels.begin(), s.rels.end(), jp.inner_rel) != s.rels.end() && S.delta_n != 0) return false;
+
+    // geometry: one bit matrix per instance, rows = its values
+    const u64 rows = p->max_value + 1;
+    const u32 ninst = std::max<u32>(p->n_inst, 1);
+    std::vector<DenseInst> hi(ninst);
+    u64 words = 0, wmax = 1;
+    for (u32 i = 0; i < ninst; i++) {
+        const u64 b = p->n_inst ? p->inst_base_h[i] : 0;
+        const u64 e = (p->n_inst && i + 1 < p->n_inst) ? p->inst_base_h[i + 1] : rows;
+        const u64 n = e > b ? e - b : 1;
+        if (n > kDenseMaxN) return false;
+        hi[i] = DenseInst{b, n, (n + 31) / 32, words};
+        words += n * hi[i].words;
+        wmax = std::max(wmax, hi[i].words);
+    }
+    if (2.0 * 4.0 * (double)words + 16.0 * (double)rows > p->tune.dense_max_bytes) return false;
+
+    DenseBufs B(p);
+    dev_alloc(p, &B.known, words);
+    dev_alloc(p, &B.delta0, words);
+    dev_alloc(p, &B.row_new, rows);
+    dev_alloc(p, &B.row_off, rows);
+    dev_alloc(p, &B.counters, 4);
+    dev_alloc(p, &B.flags, 1);
+    dev_alloc(p, &B.inst, ninst);
+    CK(cudaMemcpyAsync(B.inst, hi.data(), ninst * sizeof(DenseInst), cudaMemcpyHostToDevice, p->stream));
+    const u64 *sk, *sv;
+    u64 sn;
+    version_rows(p, S, RA_FULL, &sk, &sv, &sn);
+    const u64* scsr = version_csr(p, S, RA_FULL);
+    const u64 n_stored = R.full_n + R.delta_n;
+    const size_t smem = 3 * wmax * sizeof(u32);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_closure_kernel, kThreads, smem));
+    const int grid = kSms * std::max(per_sm, 1);
+
+    u64 level_cap = 256;
+    std::vector<u64> hflags(2);
+    for (;;) {
+        dev_free(p, &B.level_total);
+        dev_alloc(p, &B.level_total, level_cap);
+        if (p->n_inst) {
+            size_instance_rows(p, level_cap);
+            CK(cudaMemsetAsync(p->dinst_new, 0, p->inst_rows_cap * p->n_inst * 8, p->stream));
+        }
+        CK(cudaMemsetAsync(B.known, 0, words * 4, p->stream));
+        CK(cudaMemsetAsync(B.delta0, 0, words * 4, p->stream));
+        CK(cudaMemsetAsync(B.row_new, 0, rows * 8, p->stream));
+        CK(cudaMemsetAsync(B.level_total, 0, level_cap * 8, p->stream));
+        CK(cudaMemsetAsync(B.counters, 0, 4 * 8, p->stream));
+        CK(cudaMemsetAsync(B.flags, 0, 4, p->stream));
+        DenseArgs a{};
+        a.inst = B.inst;
+        a.inst_base = p->n_inst ? p->dinst_base : nullptr;
+        a.n_inst = ninst;
+        a.rows = rows;
+        a.known = B.known;
+        a.delta0 = B.delta0;
+        a.bits = p->bits;
+        a.s_keys = sk;
+        a.s_csr = scsr;
+        a.row_new = B.row_new;
+        a.level_total = B.level_total;
+        a.inst_level = p->n_inst ? p->dinst_new : nullptr;
+        a.level_cap = p->n_inst ? std::min(level_cap, p->inst_rows_cap) : level_cap;
+        a.counters = B.counters;
+        a.flags = B.flags;
+        if (n_stored) {
+            dense_load_kernel<<<grid_for(n_stored), kThreads, 0, p->stream>>>(a, R.keys, R.full_n, n_stored);
+            LAUNCHED();
+        }
+        dense_closure_kernel<<<grid, kThreads, smem, p->stream>>>(a, (u32)wmax);
+        LAUNCHED();
+        u32 fl = 0;
+        CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        if (fl & kDenseFlagRange)
+            fail(p, RA_E_BADARG, "SCC %d: a value of %s or %s lies outside its instance's range", s.id,
+                 R.name.c_str(), S.name.c_str());
+        if (!(fl & kDenseFlagLevels)) {
+            level_cap = a.level_cap;
+            break;
+        }
+        level_cap *= 4;   // a deeper search than the level arrays held: again with room
+        p->stats.regrows++;
+    }
+
+    // new tuples, row by row, after R's stored ones
+    const u64 total = scan_exclusive<u64>(p, B.row_new, rows, B.row_off);
+    u64& ctr = intern_counter(p, R.tag);
+    if (total) {
+        ensure_log(p, R, n_stored + total);
+        dense_emit_kernel<<<std::min<u64>(rows, (u64)kSms * 16), kThreads, 0, p->stream>>>(
+            DenseArgs{B.inst, p->n_inst ? p->dinst_base : nullptr, ninst, rows, B.known, B.delta0, p->bits, sk, scsr,
+                      B.row_new, B.level_total, nullptr, level_cap, B.counters, B.flags},
+            B.row_off, R.keys + n_stored, R.ids + n_stored, (u64)R.tag << 46, ctr);
+        LAUNCHED();
+    }
+    std::vector<u64> lv(level_cap), cnt(4);
+    CK(cudaMemcpyAsync(lv.data(), B.level_total, level_cap * 8, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(cnt.data(), B.counters, 4 * 8, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    u64 L = 0;
+    while (L < level_cap && lv[L]) L++;
+    const u64 iterations = L + 1;   // the last one finds nothing new
+    if (p->n_inst) {
+        const size_t at = p->inst_hist.size();
+        p->inst_hist.resize(at + (size_t)iterations * p->n_inst);
+        CK(cudaMemcpyAsync(p->inst_hist.data() + at, p->dinst_new, (size_t)iterations * p->n_inst * 8,
+                           cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+    }
+
+    // history: the semi-naive bookkeeping of every iteration (end_of_iteration's)
+    std::vector<u64> f(s.rels.size()), d(s.rels.size());
+    for (size_t i = 0; i < s.rels.size(); i++) {
+        f[i] = p->rels[s.rels[i]].full_n;
+        d[i] = p->rels[s.rels[i]].delta_n;
+    }
+    std::vector<uint64_t> hist;
+    for (u64 k = 0; k < iterations; k++) {
+        u64 sd = 0, sf = 0;
+        for (size_t i = 0; i < s.rels.size(); i++) {
+            f[i] += d[i];
+            d[i] = (s.rels[i] == ru.out && k < L) ? lv[k] : 0;
+            sd += d[i];
+            sf += f[i];
+        }
+        hist.push_back(sd);
+        hist.push_back(sf);
+    }
+    p->history.push_back((uint64_t)s.id);
+    p->history.push_back(iterations);
+    p->history.insert(p->history.end(), hist.begin(), hist.end());
+
+    // the log is [old full | old delta | new]: sorted only when a single sorted region holds it all
+    const bool sorted = total == 0 && ((R.delta_n == 0 && R.full_sorted) || (R.full_n == 0 && R.delta_sorted));
+    ctr += total;
+    R.full_n = n_stored + total;
+    R.delta_n = 0;
+    R.newt_n = 0;
+    R.full_sorted = sorted;
+    R.delta_sorted = true;
+    R.full_version = fresh_stamp();
+    R.delta_version = fresh_stamp();
+    if (R.seen) R.seen_dirty = true;   // the hash set holds none of the new tuples
+    p->stats.iterations += iterations;
+    p->stats.new_tuples += total;
+    p->stats.join_candidates += cnt[1];
+    p->stats.dense_sccs++;
+    return true;
+}
+
 void run_scc(ra_program* p, Scc& s)
 {
     for (const Rule& ru : s.rules)
@@ -1403,6 +1603,10 @@ void run_scc(ra_program* p, Scc& s)
                  p->rels[ru.out].name.c_str());
     for (size_t i = 0; i < s.rels.size(); i++)
         if (s.init[i]) full_to_delta(p, p->rels[s.rels[i]]);
+    if (run_scc_dense(p, s)) {
+        for (int ri : s.rels) delta_to_full(p->rels[ri]);
+        return;
+    }
     {
         DevScc d;
         if (build_dev_scc(p, s, d)) {
@@ -1453,6 +1657,7 @@ void choose_bits(ra_program* p)
                  "relation %s: %u columns of %d bits do not pack into one 63-bit key (largest value %llu)",
                  r.name.c_str(), r.arity, bits, (unsigned long long)mx);
     p->bits = bits;
+    p->max_value = mx;
 }
 
 void free_relation_state(ra_program* p, Relation& r)
@@ -2014,6 +2219,7 @@ int ra_program_set_tuning(ra_program* p, const ra_tuning* t)
         if (t->join_blocks_per_sm < 1 || t->join_blocks_per_sm > 16 || t->select_blocks_per_sm < 1 ||
             t->select_blocks_per_sm > 16)
             fail(p, RA_E_BADARG, "blocks per SM outside [1, 16]");
+        if (!(t->dense_max_bytes >= 0.0 && t->dense_max_bytes <= 1e12)) fail(p, RA_E_BADARG, "dense_max_bytes outside [0, 1e12]");
         p->tune = *t;
     });
 }

@@ -51,7 +51,7 @@ class Stats(C.Structure):
         ("dedup_launches", C.c_uint64), ("dedup_bytes", C.c_uint64), ("value_bits", C.c_uint32),
         ("reserved", C.c_uint32), ("phase_ms", C.c_double * 6), ("graph_builds", C.c_uint64),
         ("graph_build_ms", C.c_double), ("regrows", C.c_uint64), ("device_bytes", C.c_uint64),
-        ("device_bytes_peak", C.c_uint64),
+        ("device_bytes_peak", C.c_uint64), ("dense_sccs", C.c_uint64),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 
@@ -60,9 +60,10 @@ class Tuning(C.Structure):
     """ra_tuning: hash load factor, growth factors and kernel grid shapes of a program."""
     _fields_ = [
         ("seen_load_max", C.c_double), ("seen_grow", C.c_double), ("log_growth", C.c_double),
-        ("join_blocks_per_sm", C.c_uint32), ("select_blocks_per_sm", C.c_uint32),
+        ("join_blocks_per_sm", C.c_uint32), ("select_blocks_per_sm", C.c_uint32), ("dense_max_bytes", C.c_double),
     ]
-    FIELDS = ("seen_load_max", "seen_grow", "log_growth", "join_blocks_per_sm", "select_blocks_per_sm")
+    FIELDS = ("seen_load_max", "seen_grow", "log_growth", "join_blocks_per_sm", "select_blocks_per_sm",
+              "dense_max_bytes")
 
     def as_dict(self):
         return {k: getattr(self, k) for k in self.FIELDS}

@@ -16,7 +16,7 @@ def test_tuning_round_trip_and_validation():
     t2 = p.get_tuning()
     assert abs(t2["seen_load_max"] - 0.7) < 1e-12 and t2["join_blocks_per_sm"] == 2
     for bad in ({"seen_load_max": 0.95}, {"seen_load_max": 0.05}, {"seen_grow": 1.0}, {"log_growth": 5.0},
-                {"join_blocks_per_sm": 0}, {"select_blocks_per_sm": 17}):
+                {"join_blocks_per_sm": 0}, {"select_blocks_per_sm": 17}, {"dense_max_bytes": -1.0}):
         with pytest.raises(P.RAError):
             p.set_tuning(**bad)
     assert p.get_tuning() == t2
