@@ -395,8 +395,10 @@ def run_batched(args, rank, world, local_rank):
     free, _ = torch.cuda.mem_get_info(local_rank)
     budget = args.wave_tuples or min(P.batch.WAVE_TUPLES, 0.5 * free / P.batch.BYTES_PER_TUPLE)
     spans = [value_span(insts[i]) for i in order]
+    # waves within the tuple budget, the 30-bit join-key range and the dense evaluator's bit matrices
     waves = [[int(order[j]) for j in w] for w in plan_waves(est[order], budget, max_values=(1 << 30) - 1,
-                                                             spans=spans)]
+                                                             spans=spans,
+                                                             max_dense_bytes=0.9 * P.batch.DENSE_MAX_BYTES)]
     stream = torch.cuda.Stream()
     runner = Runner("tc", local_rank)
     runner.prog.set_stream(stream.cuda_stream)

@@ -34,6 +34,16 @@ from .programs import PROGRAMS
 _TUNED = tuning_file() or {}
 BYTES_PER_TUPLE = float(_TUNED.get("bytes_per_tuple", 160.0))
 WAVE_TUPLES = float(_TUNED.get("wave_tuples", 3e8))
+# The engine's dense row-closure evaluator (transitive-closure-shaped SCCs):
+# instances of at most DENSE_MAX_N values, bit matrices within DENSE_MAX_BYTES
+# (ra_tuning.dense_max_bytes; a wave beyond it runs on the hash-set path).
+DENSE_MAX_N = 65536
+DENSE_MAX_BYTES = float((_TUNED.get("tuning") or {}).get("dense_max_bytes", 8e9))
+
+
+def dense_bytes(span: int) -> float:
+    """Device bytes of one instance's bit matrices (known + initial delta) and row counters."""
+    return 2.0 * span * ((span + 31) // 32) * 4 + 16.0 * span
 
 
 @dataclass
@@ -124,22 +134,27 @@ def estimate_tuples(kind: str, rows: np.ndarray) -> float:
     return n / max(1.0 - d, 1.0 / math.sqrt(n)) + m
 
 
-def plan_waves(estimates, budget_tuples: float, max_values: int | None = None, spans=None):
+def plan_waves(estimates, budget_tuples: float, max_values: int | None = None, spans=None,
+               max_dense_bytes: float | None = None):
     """Split instance indices into waves whose estimated tuples stay within budget.
 
     Instances are taken in the given order; a wave closes when the next
     instance would overflow the budget (a single instance above it gets a wave
-    of its own) or, with ``max_values``, the union's value range.
+    of its own), or, with ``max_values``, the union's value range, or, with
+    ``max_dense_bytes``, the bit matrices of the dense evaluator.
     """
-    waves, cur, tot, vals = [], [], 0.0, 0
+    waves, cur, tot, vals, dense = [], [], 0.0, 0, 0.0
     for i, e in enumerate(estimates):
         sp = spans[i] if spans is not None else 0
-        if cur and (tot + e > budget_tuples or (max_values is not None and vals + sp > max_values)):
+        db = dense_bytes(sp) if max_dense_bytes is not None else 0.0
+        if cur and (tot + e > budget_tuples or (max_values is not None and vals + sp > max_values)
+                    or (max_dense_bytes is not None and dense + db > max_dense_bytes)):
             waves.append(cur)
-            cur, tot, vals = [], 0.0, 0
+            cur, tot, vals, dense = [], 0.0, 0, 0.0
         cur.append(i)
         tot += e
         vals += sp
+        dense += db
     if cur:
         waves.append(cur)
     return waves
@@ -187,15 +202,25 @@ class Runner:
     def union_rows(rows_list):
         """(union rows, value bases): instance i's data columns shifted by base[i]."""
         k = len(rows_list)
-        spans = np.fromiter((value_span(r) for r in rows_list), dtype=np.uint64, count=k)
         base = np.zeros(k, dtype=np.uint64)
-        if k > 1:
-            base[1:] = np.cumsum(spans[:-1])
         if not k:
             return np.empty((0, 3), dtype=np.uint64), base
-        union = np.concatenate(rows_list).astype(np.uint64, copy=False)
         sizes = np.fromiter((r.shape[0] for r in rows_list), dtype=np.int64, count=k)
-        union[:, :-1] += np.repeat(base, sizes)[:, None]
+        union = np.concatenate(rows_list).astype(np.uint64, copy=False)
+        # span of each instance: 1 + its largest data value (1 for an empty instance)
+        spans = np.ones(k, dtype=np.uint64)
+        nz = np.flatnonzero(sizes)
+        if nz.size:
+            row_max = union[:, 0].copy()
+            for c in range(1, union.shape[1] - 1):
+                np.maximum(row_max, union[:, c], out=row_max)
+            starts = (np.cumsum(sizes) - sizes)[nz]
+            spans[nz] = np.maximum.reduceat(row_max, starts) + np.uint64(1)
+        if k > 1:
+            base[1:] = np.cumsum(spans[:-1])
+        shift = np.repeat(base, sizes)
+        for c in range(union.shape[1] - 1):
+            union[:, c] += shift
         return union, base
 
     def load_wave(self, rows_list) -> np.ndarray:

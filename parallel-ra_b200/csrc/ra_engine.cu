@@ -1406,7 +1406,10 @@ struct DenseBufs {
     u64* level_total = nullptr;
     u64* counters = nullptr;
     u32* flags = nullptr;
+    u32* s_local = nullptr;
     DenseInst* inst = nullptr;
+    DenseChunk* chunks = nullptr;
+    u64* inst_init = nullptr;
     explicit DenseBufs(ra_program* pp) : p(pp) {}
     ~DenseBufs()
     {
@@ -1417,7 +1420,10 @@ struct DenseBufs {
         dev_free(p, &level_total);
         dev_free(p, &counters);
         dev_free(p, &flags);
+        dev_free(p, &s_local);
         dev_free(p, &inst);
+        dev_free(p, &chunks);
+        dev_free(p, &inst_init);
     }
 };
 
@@ -1447,7 +1453,7 @@ bool run_scc_dense(ra_program* p, Scc& s)
     const u64 rows = p->max_value + 1;
     const u32 ninst = std::max<u32>(p->n_inst, 1);
     std::vector<DenseInst> hi(ninst);
-    u64 words = 0, wmax = 1;
+    u64 words = 0;
     for (u32 i = 0; i < ninst; i++) {
         const u64 b = p->n_inst ? p->inst_base_h[i] : 0;
         const u64 e = (p->n_inst && i + 1 < p->n_inst) ? p->inst_base_h[i + 1] : rows;
@@ -1455,7 +1461,6 @@ bool run_scc_dense(ra_program* p, Scc& s)
         if (n > kDenseMaxN) return false;
         hi[i] = DenseInst{b, n, (n + 31) / 32, words};
         words += n * hi[i].words;
-        wmax = std::max(wmax, hi[i].words);
     }
     if (2.0 * 4.0 * (double)words + 16.0 * (double)rows > p->tune.dense_max_bytes) return false;
 
@@ -1464,20 +1469,18 @@ bool run_scc_dense(ra_program* p, Scc& s)
     dev_alloc(p, &B.delta0, words);
     dev_alloc(p, &B.row_new, rows);
     dev_alloc(p, &B.row_off, rows);
-    dev_alloc(p, &B.counters, 4);
+    dev_alloc(p, &B.counters, 8);
     dev_alloc(p, &B.flags, 1);
     dev_alloc(p, &B.inst, ninst);
+    dev_alloc(p, &B.inst_init, ninst);
+    constexpr int kShapes = 4;   // search kernels: warp per row with 1, 4, 16 words per lane; CTA per row
     CK(cudaMemcpyAsync(B.inst, hi.data(), ninst * sizeof(DenseInst), cudaMemcpyHostToDevice, p->stream));
     const u64 *sk, *sv;
     u64 sn;
     version_rows(p, S, RA_FULL, &sk, &sv, &sn);
     const u64* scsr = version_csr(p, S, RA_FULL);
+    dev_alloc(p, &B.s_local, sn);
     const u64 n_stored = R.full_n + R.delta_n;
-    const size_t smem = 3 * wmax * sizeof(u32);
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_closure_kernel, kThreads, smem));
-    const int grid = kSms * std::max(per_sm, 1);
-
     u64 level_cap = 256;
     std::vector<u64> hflags(2);
     for (;;) {
@@ -1491,8 +1494,9 @@ bool run_scc_dense(ra_program* p, Scc& s)
         CK(cudaMemsetAsync(B.delta0, 0, words * 4, p->stream));
         CK(cudaMemsetAsync(B.row_new, 0, rows * 8, p->stream));
         CK(cudaMemsetAsync(B.level_total, 0, level_cap * 8, p->stream));
-        CK(cudaMemsetAsync(B.counters, 0, 4 * 8, p->stream));
+        CK(cudaMemsetAsync(B.counters, 0, 8 * 8, p->stream));
         CK(cudaMemsetAsync(B.flags, 0, 4, p->stream));
+        CK(cudaMemsetAsync(B.inst_init, 0, ninst * 8, p->stream));
         DenseArgs a{};
         a.inst = B.inst;
         a.inst_base = p->n_inst ? p->dinst_base : nullptr;
@@ -1503,18 +1507,90 @@ bool run_scc_dense(ra_program* p, Scc& s)
         a.bits = p->bits;
         a.s_keys = sk;
         a.s_csr = scsr;
+        a.s_local = B.s_local;
         a.row_new = B.row_new;
         a.level_total = B.level_total;
         a.inst_level = p->n_inst ? p->dinst_new : nullptr;
         a.level_cap = p->n_inst ? std::min(level_cap, p->inst_rows_cap) : level_cap;
+        a.inst_init = B.inst_init;
         a.counters = B.counters;
         a.flags = B.flags;
+        if (sn) {
+            dense_local_kernel<<<grid_for(sn), kThreads, 0, p->stream>>>(a, sn);
+            LAUNCHED();
+        }
         if (n_stored) {
             dense_load_kernel<<<grid_for(n_stored), kThreads, 0, p->stream>>>(a, R.keys, R.full_n, n_stored);
             LAUNCHED();
         }
-        dense_closure_kernel<<<grid, kThreads, smem, p->stream>>>(a, (u32)wmax);
-        LAUNCHED();
+        // work: chunks of rows of one instance.  A row's search reaches about s * n values when the
+        // initial delta averages d > 1 tuples per row (s = 1 - exp(-d s), the giant component of a
+        // random graph), a handful otherwise.  Instances whose rows reach at most 2048 values (and
+        // of at most 16384 values) run one warp per row (words per lane 1, 4 or 16: three kernel
+        // shapes), with no block barriers; wider searches run one CTA per row.
+        std::vector<u64> init(ninst);
+        CK(cudaMemcpyAsync(init.data(), B.inst_init, ninst * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        auto shape_of = [&](u32 i) {
+            const u64 w = hi[i].words;
+            const double n = (double)hi[i].n, deg = (double)init[i] / n;
+            double sfrac = 0.0;
+            if (deg > 1.0) {
+                sfrac = 0.5;
+                for (int it = 0; it < 60; it++) sfrac = 1.0 - std::exp(-deg * sfrac);
+            }
+            if (w > 512 || (w > 32 && sfrac * n > 2048.0)) return 3;
+            return w <= 32 ? 0 : w <= 128 ? 1 : 2;
+        };
+        std::vector<DenseChunk> chunks;
+        u64 first[kShapes + 1] = {0};
+        u64 cta_wmax = 1;
+        for (int sh = 0; sh < kShapes; sh++) {
+            first[sh] = chunks.size();
+            for (u32 i = 0; i < ninst; i++) {
+                const DenseInst& di = hi[i];
+                if (shape_of(i) != sh || di.base >= rows) continue;
+                if (sh == 3) cta_wmax = std::max(cta_wmax, di.words);
+                const u64 cnt = std::min(di.n, rows - di.base), per = sh == 3 ? 4 : 8;
+                for (u64 r0 = 0; r0 < cnt; r0 += per)
+                    chunks.push_back(DenseChunk{di.base + r0, i, (u32)std::min(per, cnt - r0)});
+            }
+        }
+        first[kShapes] = chunks.size();
+        dev_free(p, &B.chunks);
+        dev_alloc(p, &B.chunks, std::max<size_t>(chunks.size(), 1));
+        if (!chunks.empty())
+            CK(cudaMemcpyAsync(B.chunks, chunks.data(), chunks.size() * sizeof(DenseChunk), cudaMemcpyHostToDevice,
+                               p->stream));
+        const size_t smem = 3 * cta_wmax * sizeof(u32);
+        // grids: resident CTAs of each kernel, at most one warp (CTA) per chunk
+        auto resident = [&](const void* fn, size_t dyn) {
+            int per_sm = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, dyn));
+            return (u64)kSms * (u64)std::max(per_sm, 1);
+        };
+        const void* fns[kShapes] = {(const void*)dense_closure_warp_kernel<1>, (const void*)dense_closure_warp_kernel<4>,
+                                    (const void*)dense_closure_warp_kernel<16>, (const void*)dense_closure_kernel};
+        int grids[kShapes];
+        for (int sh = 0; sh < kShapes; sh++) {
+            const u64 n = first[sh + 1] - first[sh];
+            const u64 want = sh == 3 ? n : (n + kWarps - 1) / kWarps;
+            grids[sh] = (int)std::max<u64>(1, std::min(resident(fns[sh], sh == 3 ? smem : 0), want));
+        }
+        // one chunk counter per shape: counters[0] and [2] .. [4]
+        u64* ctr[kShapes] = {B.counters + 2, B.counters + 3, B.counters + 4, B.counters};
+        const u64 nc[kShapes] = {first[1] - first[0], first[2] - first[1], first[3] - first[2], first[4] - first[3]};
+        if (nc[0])
+            dense_closure_warp_kernel<1><<<grids[0], kThreads, 0, p->stream>>>(a, B.chunks + first[0], nc[0], ctr[0]);
+        if (nc[1])
+            dense_closure_warp_kernel<4><<<grids[1], kThreads, 0, p->stream>>>(a, B.chunks + first[1], nc[1], ctr[1]);
+        if (nc[2])
+            dense_closure_warp_kernel<16><<<grids[2], kThreads, 0, p->stream>>>(a, B.chunks + first[2], nc[2], ctr[2]);
+        if (nc[3])
+            dense_closure_kernel<<<grids[3], kThreads, smem, p->stream>>>(a, (u32)cta_wmax, B.chunks + first[3], nc[3],
+                                                                          ctr[3]);
+        for (int sh = 0; sh < kShapes; sh++)
+            if (nc[sh]) LAUNCHED();
         u32 fl = 0;
         CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
         CK(cudaStreamSynchronize(p->stream));
@@ -1534,9 +1610,9 @@ bool run_scc_dense(ra_program* p, Scc& s)
     u64& ctr = intern_counter(p, R.tag);
     if (total) {
         ensure_log(p, R, n_stored + total);
-        dense_emit_kernel<<<std::min<u64>(rows, (u64)kSms * 16), kThreads, 0, p->stream>>>(
+        dense_emit_kernel<<<std::min<u64>((rows + kWarps - 1) / kWarps, (u64)kSms * 16), kThreads, 0, p->stream>>>(
             DenseArgs{B.inst, p->n_inst ? p->dinst_base : nullptr, ninst, rows, B.known, B.delta0, p->bits, sk, scsr,
-                      B.row_new, B.level_total, nullptr, level_cap, B.counters, B.flags},
+                      B.s_local, B.row_new, B.level_total, nullptr, level_cap, B.inst_init, B.counters, B.flags},
             B.row_off, R.keys + n_stored, R.ids + n_stored, (u64)R.tag << 46, ctr);
         LAUNCHED();
     }

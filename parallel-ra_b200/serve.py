@@ -34,7 +34,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import batch
-from .batch import Runner, estimate_tuples
+from .batch import DENSE_MAX_BYTES, DENSE_MAX_N, Runner, dense_bytes, estimate_tuples, value_span
 from .engine import E_OOM, RAError
 
 
@@ -45,6 +45,7 @@ class Request:
     rows: np.ndarray
     arrival: float = 0.0              # seconds after the stream's start (scheduled)
     est_tuples: float = 0.0
+    span: int = 0                     # values the instance occupies
     submitted: float | None = None    # perf_counter at submission
     started: float | None = None      # its wave's start
     done: float | None = None         # its wave's end (results available)
@@ -105,6 +106,8 @@ class Server:
     def submit(self, req: Request) -> None:
         if not req.est_tuples:
             req.est_tuples = estimate_tuples(req.kind, req.rows)
+        if not req.span:
+            req.span = value_span(req.rows)
         req.submitted = time.perf_counter()
         with self._cv:
             self._queue.append(req)
@@ -134,6 +137,13 @@ class Server:
                 r.close()
 
     # ------------------------------------------------------------------ workers
+    @staticmethod
+    def _cls(req: Request):
+        """Requests that share a wave: same program, and for ``tc`` the same side of
+        the dense evaluator's size limit (one large instance would send the
+        whole wave to the hash-set path)."""
+        return req.kind, req.kind == "tc" and req.span <= DENSE_MAX_N
+
     def _mem(self, req: Request) -> float:
         return req.est_tuples * self.correction[req.kind] * self.bpt[req.kind]
 
@@ -151,6 +161,8 @@ class Server:
         if not self._queue or (self._exclusive is not None and self._exclusive != w):
             return None
         kind = self._queue[0].kind
+        cls = self._cls(self._queue[0])
+        dense_cap = 0.9 * DENSE_MAX_BYTES if cls[1] else None
         held = self._used[w]
         first = self._mem(self._queue[0])
         others = sum(u for i, u in enumerate(self._used) if i != w)
@@ -160,18 +172,21 @@ class Server:
             self._release_idle(w)      # only idle buffers stand in the way
             others = 0.0
         free = self.budget - others
-        picked, est, mem = [], 0.0, 0.0
+        picked, est, mem, dense = [], 0.0, 0.0, 0.0
         for req in self._queue:
-            if req.kind != kind:
+            if self._cls(req) != cls:
                 continue
             m = self._mem(req)
             e = req.est_tuples * self.correction[kind]
+            db = dense_bytes(req.span) if dense_cap is not None else 0.0
             if picked and (est + e > self.wave_tuples or max(held, mem + m) > free
-                           or len(picked) >= self.max_wave_requests):
+                           or len(picked) >= self.max_wave_requests
+                           or (dense_cap is not None and dense + db > dense_cap)):
                 break
             picked.append(req)         # the first one always (alone it may exceed an empty budget)
             est += e
             mem += m
+            dense += db
         taken = set(id(r) for r in picked)
         self._queue = collections.deque(r for r in self._queue if id(r) not in taken)
         self._used[w] = max(held, mem)
@@ -326,6 +341,8 @@ def run_stream(server: Server, reqs: list[Request], arrivals: np.ndarray, timeou
         r.arrival = float(a)
         if not r.est_tuples:
             r.est_tuples = estimate_tuples(r.kind, r.rows)
+        if not r.span:
+            r.span = value_span(r.rows)
     base_done = len(server.completed)
     t0 = time.perf_counter()
     for r in reqs:

@@ -174,3 +174,11 @@ def test_set_instances_rejects_unordered_bases():
     with pytest.raises(P.RAError):
         p.instance_history()
     p.close()
+
+
+def test_plan_waves_respects_dense_bytes():
+    from parallel_ra_b200.batch import dense_bytes
+    spans = [1000, 1000, 1000, 5000]
+    cap = 2.5 * dense_bytes(1000)
+    waves = plan_waves([1, 1, 1, 1], budget_tuples=1e9, spans=spans, max_dense_bytes=cap)
+    assert waves == [[0, 1], [2], [3]]

@@ -7,8 +7,8 @@ import parallel_ra_b200 as P
 from parallel_ra_b200.serve import Request, Server, poisson_arrivals, request_mix, run_stream
 
 
-def fake(rid, kind, est):
-    return Request(rid, kind, np.empty((0, 3), dtype=np.uint64), est_tuples=est)
+def fake(rid, kind, est, span=100):
+    return Request(rid, kind, np.empty((0, 3), dtype=np.uint64), est_tuples=est, span=span)
 
 
 def test_admission_takes_oldest_kind_in_order_within_budget():
@@ -109,3 +109,13 @@ def test_oom_retry_waits_for_others_and_runs_alone():
     for _, w, busy in starts:                  # nobody else was busy while a retry ran
         assert not busy[1 - w]
     assert s._exclusive is None and s.oom_retries == 2
+
+
+def test_large_tc_requests_wave_apart_from_dense_ones():
+    s = Server(slots=1, budget_bytes=1e12, wave_tuples=1e9, bytes_per_tuple=1, start=False)
+    s._queue.extend([fake(0, "tc", 1), fake(1, "tc", 1, span=1 << 18), fake(2, "tc", 1), fake(3, "tc", 1, span=1 << 18)])
+    _, picked, _ = s._take_wave(0)
+    assert [r.rid for r in picked] == [0, 2]
+    s._busy[0] = False
+    _, picked, _ = s._take_wave(0)
+    assert [r.rid for r in picked] == [1, 3]
