@@ -45,6 +45,8 @@ WORKLOADS = {
     "tc-er20": ("tc", "er", (1 << 20, 996147, 2)),    # same family at 1/4 scale (profiling case)
     "tc-er2000": ("tc", "er", (2000, 3000, 1)),
     "sg-tree15": ("sg", "tree", (1 << 15, 3)),         # same generation on a random tree of 2^15 nodes
+    # the largest instance class of the batched mix: a dense closure (dense row-closure evaluator)
+    "tc-er16384d2": ("tc", "er", (16384, 32768, 7)),
 }
 OUTPUT = {"tc": "T", "sg": "SG"}
 INPUT = {"tc": "G", "sg": "edge"}
@@ -52,10 +54,10 @@ INPUT = {"tc": "G", "sg": "edge"}
 CPU_SAMPLES = {"tc": ("er", (1 << 17, round(0.95 * (1 << 17)), 2)), "sg": ("tree", (1 << 12, 3))}
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
-# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.79 / 1.81 / 1.83 over
+# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.86 / 1.87 / 1.87 over
 # three launches of the same graph family at 1/4 scale); bench's `traffic` is
 # this ratio times the algorithmic bytes of an average tc-er22 launch.
-TRAFFIC_PER_ALGO_BYTE = 1.81
+TRAFFIC_PER_ALGO_BYTE = 1.87
 
 
 def load_peaks():
@@ -167,6 +169,34 @@ def cpu_sample_desc(kind="tc"):
     return f"SG on a random tree of n={n} nodes seed={s} (same family as the workload), fixpoint time only"
 
 
+def accumulate_dense(acc, st):
+    """Add a run's dense-evaluator figures (filled with per-launch timing) to ``acc``."""
+    if st.dense_sccs:
+        acc["search_ms"] += st.dense_search_ms
+        acc["emit_ms"] += st.dense_emit_ms
+        acc["sccs"] += st.dense_sccs
+        acc["new_tuples"] += st.new_tuples
+        acc["candidates"] += st.join_candidates
+
+
+def dense_roofline(d, peak, peak_kind):
+    """Roofline of the dense row-closure evaluator's kernels.  The emission kernel is
+    HBM-bound: 16 B written per new tuple (key + id).  The row searches run in shared
+    memory against an L2-resident adjacency; their bound is SM issue, not DRAM, so they
+    are reported with their time share and edge rate beside the HBM roofline."""
+    achieved = 16.0 * d["new_tuples"] / (d["emit_ms"] / 1e3) / 1e9 if d["emit_ms"] else 0.0
+    tot = d["search_ms"] + d["emit_ms"]
+    return {"kernel": "dense_emit_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "bytes_model": "16 B written per new tuple (key + id)",
+            "share_of_dense_time": d["emit_ms"] / tot if tot else None,
+            "dense_search": {"kernels": "dense_closure_kernel / dense_closure_warp_kernel", "ms": d["search_ms"],
+                             "share_of_dense_time": d["search_ms"] / tot if tot else None,
+                             "edges_per_s": d["candidates"] / (d["search_ms"] / 1e3) if d["search_ms"] else None,
+                             "bound": "SM issue: shared-memory bit sets and atomics, adjacency L2-resident "
+                                      "(ncu: sm__throughput ~73%, DRAM idle)"}}
+
+
 def metric_of(kind):
     return f"{OUTPUT[kind]} tuples/s" if kind == "sg" else METRIC
 
@@ -270,6 +300,7 @@ def run_ours(args, rank, world, local_rank):
     prog.set_launch_timing(True)
     dedup_ms = dedup_bytes = dedup_launches = 0
     phase = [0.0] * 6
+    dense = {"search_ms": 0.0, "emit_ms": 0.0, "sccs": 0, "new_tuples": 0, "candidates": 0}
     for _ in range(max(1, min(args.steps, 3))):
         prog.execute(1)
         s2 = prog.stats()
@@ -277,6 +308,7 @@ def run_ours(args, rank, world, local_rank):
         dedup_bytes += s2.dedup_bytes
         dedup_launches += s2.dedup_launches
         phase = [a + b for a, b in zip(phase, s2.phase_ms)]
+        accumulate_dense(dense, s2)
     prog.set_launch_timing(False)
 
     # the same program with intern ids numbered exactly as the single-rank reference
@@ -310,7 +342,7 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = load_peaks()
     achieved = (dedup_bytes / dedup_launches) / ((dedup_ms / dedup_launches) / 1e3) / 1e9 if dedup_launches else 0.0
-    roofline = {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roofline = dense_roofline(dense, peak, peak_kind) if dense["sccs"] else {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": TRAFFIC_PER_ALGO_BYTE * dedup_bytes / max(dedup_launches, 1),
                 "traffic_note": "ncu DRAM read+write per launch, measured on tc-er20 and scaled by units processed",
@@ -445,15 +477,21 @@ def run_batched(args, rank, world, local_rank):
     runner.run_wave_resident(base, t.data_ptr(), nrows)
     s2 = runner.prog.stats()
     runner.prog.set_launch_timing(False)
+    dense = {"search_ms": 0.0, "emit_ms": 0.0, "sccs": 0, "new_tuples": 0, "candidates": 0}
+    accumulate_dense(dense, s2)
     peak_bw, peak_kind = load_peaks()
     achieved = (s2.dedup_bytes / s2.dedup_launches) / ((s2.dedup_ms / s2.dedup_launches) / 1e3) / 1e9 \
         if s2.dedup_launches else 0.0
-    roofline = {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak_bw, "unit": "GB/s",
-                "frac": achieved / peak_bw, "peak_kind": peak_kind,
-                "traffic": TRAFFIC_PER_ALGO_BYTE * s2.dedup_bytes / max(s2.dedup_launches, 1),
-                "traffic_note": "ncu DRAM read+write per algorithmic byte measured on tc-er20, times this "
-                                "wave's algorithmic bytes per launch",
-                "launches": int(s2.dedup_launches), "wave": "largest wave", "instances_in_wave": len(w)}
+    if dense["sccs"]:
+        roofline = dense_roofline(dense, peak_bw, peak_kind)
+        roofline.update({"wave": "largest wave", "instances_in_wave": len(w)})
+    else:
+        roofline = {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak_bw,
+                    "unit": "GB/s", "frac": achieved / peak_bw, "peak_kind": peak_kind,
+                    "traffic": TRAFFIC_PER_ALGO_BYTE * s2.dedup_bytes / max(s2.dedup_launches, 1),
+                    "traffic_note": "ncu DRAM read+write per algorithmic byte measured on tc-er20, times this "
+                                    "wave's algorithmic bytes per launch",
+                    "launches": int(s2.dedup_launches), "wave": "largest wave", "instances_in_wave": len(w)}
     # end to end from host arrays: rebasing, upload, waves, per-instance results
     torch.cuda.synchronize()
     t0 = time.perf_counter()

@@ -98,6 +98,10 @@ typedef struct ra_stats {
     uint64_t device_bytes;      /* device memory the program holds after the run */
     uint64_t device_bytes_peak; /* most device memory it held during the run */
     uint64_t dense_sccs;        /* SCCs run by the dense row-closure evaluator */
+    /* Dense evaluator, with per-launch events only (ra_program_set_launch_timing):
+     * device time of the row searches and of the emission of new tuples. */
+    double dense_search_ms;
+    double dense_emit_ms;
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose

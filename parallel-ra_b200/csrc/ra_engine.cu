@@ -1525,7 +1525,7 @@ bool run_scc_dense(ra_program* p, Scc& s)
         }
         // work: chunks of rows of one instance.  A row's search reaches about s * n values when the
         // initial delta averages d > 1 tuples per row (s = 1 - exp(-d s), the giant component of a
-        // random graph), a handful otherwise.  Instances whose rows reach at most 2048 values (and
+        // random graph), a handful otherwise.  Instances whose rows reach at most 1024 values (and
         // of at most 16384 values) run one warp per row (words per lane 1, 4 or 16: three kernel
         // shapes), with no block barriers; wider searches run one CTA per row.
         std::vector<u64> init(ninst);
@@ -1539,7 +1539,7 @@ bool run_scc_dense(ra_program* p, Scc& s)
                 sfrac = 0.5;
                 for (int it = 0; it < 60; it++) sfrac = 1.0 - std::exp(-deg * sfrac);
             }
-            if (w > 512 || (w > 32 && sfrac * n > 2048.0)) return 3;
+            if (w > 512 || (w > 32 && sfrac * n > 1024.0)) return 3;
             return w <= 32 ? 0 : w <= 128 ? 1 : 2;
         };
         std::vector<DenseChunk> chunks;
@@ -1577,6 +1577,12 @@ bool run_scc_dense(ra_program* p, Scc& s)
             const u64 want = sh == 3 ? n : (n + kWarps - 1) / kWarps;
             grids[sh] = (int)std::max<u64>(1, std::min(resident(fns[sh], sh == 3 ? smem : 0), want));
         }
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        if (p->kernel_events) {
+            CK(cudaEventCreate(&ev[0]));
+            CK(cudaEventCreate(&ev[1]));
+            CK(cudaEventRecord(ev[0], p->stream));
+        }
         // one chunk counter per shape: counters[0] and [2] .. [4]
         u64* ctr[kShapes] = {B.counters + 2, B.counters + 3, B.counters + 4, B.counters};
         const u64 nc[kShapes] = {first[1] - first[0], first[2] - first[1], first[3] - first[2], first[4] - first[3]};
@@ -1591,6 +1597,15 @@ bool run_scc_dense(ra_program* p, Scc& s)
                                                                           ctr[3]);
         for (int sh = 0; sh < kShapes; sh++)
             if (nc[sh]) LAUNCHED();
+        if (p->kernel_events) {
+            CK(cudaEventRecord(ev[1], p->stream));
+            CK(cudaEventSynchronize(ev[1]));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            p->stats.dense_search_ms += ms;
+            cudaEventDestroy(ev[0]);
+            cudaEventDestroy(ev[1]);
+        }
         u32 fl = 0;
         CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
         CK(cudaStreamSynchronize(p->stream));
@@ -1610,11 +1625,26 @@ bool run_scc_dense(ra_program* p, Scc& s)
     u64& ctr = intern_counter(p, R.tag);
     if (total) {
         ensure_log(p, R, n_stored + total);
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        if (p->kernel_events) {
+            CK(cudaEventCreate(&ev[0]));
+            CK(cudaEventCreate(&ev[1]));
+            CK(cudaEventRecord(ev[0], p->stream));
+        }
         dense_emit_kernel<<<std::min<u64>((rows + kWarps - 1) / kWarps, (u64)kSms * 16), kThreads, 0, p->stream>>>(
             DenseArgs{B.inst, p->n_inst ? p->dinst_base : nullptr, ninst, rows, B.known, B.delta0, p->bits, sk, scsr,
                       B.s_local, B.row_new, B.level_total, nullptr, level_cap, B.inst_init, B.counters, B.flags},
             B.row_off, R.keys + n_stored, R.ids + n_stored, (u64)R.tag << 46, ctr);
         LAUNCHED();
+        if (p->kernel_events) {
+            CK(cudaEventRecord(ev[1], p->stream));
+            CK(cudaEventSynchronize(ev[1]));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            p->stats.dense_emit_ms += ms;
+            cudaEventDestroy(ev[0]);
+            cudaEventDestroy(ev[1]);
+        }
     }
     std::vector<u64> lv(level_cap), cnt(4);
     CK(cudaMemcpyAsync(lv.data(), B.level_total, level_cap * 8, cudaMemcpyDeviceToHost, p->stream));
