@@ -125,3 +125,13 @@ def test_integration_ctypes_snippet_runs(tmp_path):
     finally:
         os.chdir(cwd)
     assert env["f"].value == 3
+
+
+@pytest.mark.gpu
+def test_integration_batch_snippet_runs():
+    """The batching example in INTEGRATION.md runs and its assertion holds."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = text.split("```python")[2].split("```", 1)[0]
+    env = {}
+    exec(compile(block, "INTEGRATION.md", "exec"), env)
+    assert len(env["results"]) == 3
