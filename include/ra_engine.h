@@ -137,6 +137,22 @@ int ra_program_create(int device, ra_program** out);
 int ra_program_destroy(ra_program* p);
 /* Bind the program to an existing CUDA stream (cudaStream_t); 0 = engine's own. */
 int ra_program_set_stream(ra_program* p, void* stream);
+/* Checkpoint dumps, LIE::enable_IO + set_output_dir + set_cp_iteration (+
+ * enable_separate_io) (src/lie/lie.h:81-105, lie.cpp:154-193): after every
+ * every_batches-th batch of each SCC (0 = never), the directory
+ * <output_dir>/checkpoint-<scc id>-<batch> receives scc_metadata (executed SCC
+ * ids) and every relation's <name>_full / <name>_delta rows in trie order with
+ * their .size files, as relation::parallel_IO writes them (separate_files:
+ * per-rank names <name>_full_0, ...).  Fixed-point SCCs then run one iteration
+ * per host round trip. */
+int ra_program_set_checkpoint(ra_program* p, const char* output_dir, uint32_t every_batches, int separate_files);
+/* Restart from a dump directory, LIE::set_restart_flag + set_restart_dir_name
+ * (lie.cpp:260-330): the SCCs listed in its scc_metadata are not run again, and
+ * every SCC that runs takes each relation's delta from <dir>/<name>_delta
+ * (<name>_delta_0 with separate_files) instead of moving full into delta.
+ * The relations' full versions come from their own files (the dump's
+ * <name>_full), as the program loads them.  dump_dir NULL or "" = no restart. */
+int ra_program_set_restart(ra_program* p, const char* dump_dir, int separate_files);
 /* Read / replace the program's tuning (RA_E_BADARG outside the ranges above;
  * RA_E_STATE during a run). */
 int ra_program_get_tuning(ra_program* p, ra_tuning* out);

@@ -26,7 +26,10 @@
 #include <cstring>
 #include <atomic>
 #include <functional>
+#include <fstream>
 #include <string>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <unordered_map>
 #include <vector>
 
@@ -193,6 +196,16 @@ struct ra_program {
     bool inst_hist_ok = true;      // false once an SCC ran without instance accounting
     u64* dhist = nullptr;
     u64 dhist_cap = 0;
+    // checkpoint dumps (LIE::write_checkpoint_dump) and restart (LIE::execute's restart path)
+    std::string cp_dir;
+    uint32_t cp_every = 0;        // dump after every cp_every-th batch of an SCC; 0: no dumps
+    bool cp_separate = false;     // per-rank file names (LIE::enable_separate_io)
+    std::string rs_dir;           // restart from this dump directory ("" : no restart)
+    bool rs_separate = false;
+    std::vector<int> executed_ids;   // SCC ids completed (the dump's scc_metadata)
+    std::vector<int> rs_skip;        // SCC ids a restart does not run again
+    int loop_counter = 0;         // batches of the running SCC (LIE::execute's loop_counter)
+    std::vector<int> pending_merge;  // relations of the last SCC whose delta still awaits full
     bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
     bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
@@ -1190,6 +1203,143 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
     return sig;
 }
 
+// ---------------------------------------------------------------------------
+// checkpoint dumps and restart loading, in the reference's layout
+// ---------------------------------------------------------------------------
+
+// One region of a relation's log as a dump file: rows (arity + 1 u64) in trie
+// order, plus its size metadata (relation::parallel_IO,
+// src/relation/balanced_hash_relation.cpp:109-430): with per-rank files the rows
+// file is written when not empty and the size file always ("<bytes/24>\n3");
+// with shared files both only when not empty ("<rows>\n<arity+1>").
+void dump_region(ra_program* p, Relation& r, const u64* keys, const u64* ids, u64 n, const std::string& path)
+{
+    std::vector<u64> host(n * (r.arity + 1));
+    if (n) {
+        u64 *tk, *tv, *rows;
+        dev_alloc(p, &tk, n);
+        dev_alloc(p, &tv, n);
+        dev_alloc(p, &rows, n * (r.arity + 1));
+        CK(cudaMemcpyAsync(tk, keys, n * 8, cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(tv, ids, n * 8, cudaMemcpyDeviceToDevice, p->stream));
+        sort_rows(p, r, tk, tv, n, r.keys_unique);
+        rows_unpack<<<grid_for(n), kThreads, 0, p->stream>>>(tk, tv, n, (int)r.arity, p->bits, rows);
+        LAUNCHED();
+        CK(cudaMemcpyAsync(host.data(), rows, host.size() * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        dev_free(p, &tk);
+        dev_free(p, &tv);
+        dev_free(p, &rows);
+    }
+    const u64 bytes = host.size() * 8;
+    const std::string file = p->cp_separate ? path + "_0" : path;
+    if (n) {
+        FILE* f = fopen(file.c_str(), "wb");
+        if (!f || fwrite(host.data(), 1, bytes, f) != bytes) {
+            if (f) fclose(f);
+            fail(p, RA_E_IO, "cannot write %s", file.c_str());
+        }
+        fclose(f);
+    }
+    if (p->cp_separate || n) {
+        FILE* f = fopen((file + ".size").c_str(), "w");
+        if (!f) fail(p, RA_E_IO, "cannot write %s.size", file.c_str());
+        if (p->cp_separate) fprintf(f, "%d\n3", (int)(bytes / 24));
+        else fprintf(f, "%d\n%d", (int)n, (int)r.arity + 1);
+        fclose(f);
+    }
+}
+
+// LIE::create_checkpoint_dump + write_checkpoint_dump (src/lie/lie.cpp:154-193):
+// directory <output>/checkpoint-<scc>-<loop counter>, the executed SCC ids,
+// every relation's full and delta.  `counts` gives (full, delta) per relation.
+void write_checkpoint(ra_program* p, int scc_id, const std::vector<std::pair<u64, u64>>& counts)
+{
+    const std::string dir = p->cp_dir + "/checkpoint-" + std::to_string(scc_id) + "-" + std::to_string(p->loop_counter);
+    mkdir(dir.c_str(), S_IRWXU | S_IRWXG | S_IROTH | S_IXOTH);
+    FILE* f = fopen((dir + "/scc_metadata").c_str(), "w");
+    if (!f) fail(p, RA_E_IO, "cannot write %s/scc_metadata", dir.c_str());
+    for (int id : p->executed_ids) fprintf(f, "%d\n", id);
+    fclose(f);
+    for (size_t i = 0; i < p->rels.size(); i++) {
+        Relation& r = p->rels[i];
+        const u64 fn = counts[i].first, dn = counts[i].second;
+        dump_region(p, r, r.keys, r.ids, fn, dir + "/" + r.name + "_full");
+        dump_region(p, r, r.keys + fn, r.ids + fn, dn, dir + "/" + r.name + "_delta");
+    }
+}
+
+// After each completed batch of SCC s (one execute_in_batches call of the reference):
+// record completion and write the dump every cp_every batches.
+void checkpoint_batch(ra_program* p, const Scc& s, bool finished, const std::vector<std::pair<u64, u64>>& counts)
+{
+    if (finished) p->executed_ids.push_back(s.id);
+    if (p->cp_every && p->loop_counter % (int)p->cp_every == 0) write_checkpoint(p, s.id, counts);
+    p->loop_counter++;
+}
+
+std::vector<std::pair<u64, u64>> host_counts(ra_program* p)
+{
+    std::vector<std::pair<u64, u64>> c;
+    for (const Relation& r : p->rels) c.push_back({r.full_n, r.delta_n});
+    return c;
+}
+
+// Restart: a relation's delta from <dir>/<name>_delta (LIE::execute, lie.cpp:300-330),
+// appended after its full version; no file, no delta.
+void load_restart_delta(ra_program* p, Relation& r)
+{
+    std::string path = p->rs_dir + "/" + r.name + "_delta";
+    if (p->rs_separate) path += "_0";
+    if (access(path.c_str(), F_OK) != 0) return;
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) fail(p, RA_E_IO, "cannot open %s", path.c_str());
+    fseek(f, 0, SEEK_END);
+    const long bytes = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    const u64 w = (r.arity + 1) * 8, n = (u64)bytes / w;
+    std::vector<u64> host(n * (r.arity + 1));
+    if (n && fread(host.data(), 1, n * w, f) != n * w) {
+        fclose(f);
+        fail(p, RA_E_IO, "short read of %s", path.c_str());
+    }
+    fclose(f);
+    for (u64 i = 0; i < n; i++)
+        for (u32 c = 0; c < r.arity; c++)
+            if (host[i * (r.arity + 1) + c] >> p->bits)
+                fail(p, RA_E_UNSUPPORTED, "%s: a value wider than the %d-bit columns of the loaded relations",
+                     path.c_str(), p->bits);
+    r.full_n += r.delta_n;   // any delta present becomes full, as the reference's trie insert would keep it
+    r.delta_n = 0;
+    if (!n) return;
+    ensure_log(p, r, r.full_n + n);
+    u64* raw;
+    dev_alloc(p, &raw, n * (r.arity + 1));
+    CK(cudaMemcpyAsync(raw, host.data(), n * w, cudaMemcpyHostToDevice, p->stream));
+    rows_pack<<<grid_for(n), kThreads, 0, p->stream>>>(raw, n, (int)r.arity, p->bits, r.keys + r.full_n,
+                                                       r.ids + r.full_n);
+    LAUNCHED();
+    CK(cudaStreamSynchronize(p->stream));
+    dev_free(p, &raw);
+    r.delta_n = n;
+    r.delta_sorted = false;
+    r.full_sorted = false;
+    r.full_version = fresh_stamp();
+    r.delta_version = fresh_stamp();
+}
+
+// A completed iteration of run_scc_device that closed a batch (a new history
+// entry): counts of the SCC's relations from the control block.
+void checkpoint_device_batch(ra_program* p, const Scc& s, const DevScc& d, u64& hist_seen)
+{
+    const IterCtl& h = *p->hctl;
+    if (h.hist_n <= hist_seen) return;
+    hist_seen = h.hist_n;
+    auto counts = host_counts(p);
+    for (int sl = 0; sl < d.plan.n_rels; sl++) counts[d.rel_of_slot[sl]] = {h.full_n[sl], h.delta_n[sl]};
+    checkpoint_batch(p, s, h.done != 0, counts);
+}
+
 void drop_graph(Scc& s)
 {
     if (s.exec) cudaGraphExecDestroy(s.exec);
@@ -1249,7 +1399,8 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     LAUNCHED();
 
     int body_kernels = 0;
-    const bool graph_mode = p->use_graphs && !p->kernel_events && s.fixpoint;
+    const bool graph_mode = p->use_graphs && !p->kernel_events && s.fixpoint && !p->cp_every;
+    u64 hist_seen = 0;   // history entries (completed batches) already checkpointed
     for (;;) {
         if (graph_mode) {
             std::vector<unsigned char> sig = graph_signature(p, d);
@@ -1339,9 +1490,11 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 CK(cudaMemsetAsync(&p->ctl->sort_hist[0][0][0], 0, sizeof(p->ctl->sort_hist), p->stream));
                 CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
             }
+            if (!replay && p->cp_every) checkpoint_device_batch(p, s, d, hist_seen);
             if (h.done) break;
             continue;
         }
+        if (p->cp_every) checkpoint_device_batch(p, s, d, hist_seen);
         if (h.done) break;
     }
     // results back into the host-side relation records
@@ -1438,6 +1591,7 @@ bool run_scc_dense(ra_program* p, Scc& s)
 {
     if (!s.fixpoint || s.rules.size() != 1 || s.rules[0].kind != kJoin) return false;
     if (p->id_order != RA_IDS_EMISSION || p->batch_size != 1 || p->tune.dense_max_bytes <= 0) return false;
+    if (p->cp_every) return false;   // checkpoints need the relations after every iteration
     const Rule& ru = s.rules[0];
     const JoinPlan jp = make_join_plan(p, ru);
     if (jp.outer_rel != ru.out || jp.outer_ver != RA_DELTA || jp.inner_ver != RA_FULL || jp.inner_rel == ru.out)
@@ -1701,23 +1855,39 @@ bool run_scc_dense(ra_program* p, Scc& s)
     return true;
 }
 
+// RAM::insert_delta_in_full of the previous SCC (lie.cpp:436): done when the next SCC
+// starts or the run ends, so that counts read between SCCs are the ones the
+// reference prints there (its size print precedes the merge).
+void merge_pending(ra_program* p)
+{
+    for (int ri : p->pending_merge) delta_to_full(p->rels[ri]);
+    p->pending_merge.clear();
+}
+
 void run_scc(ra_program* p, Scc& s)
 {
+    merge_pending(p);
     for (const Rule& ru : s.rules)
         if (std::find(s.rels.begin(), s.rels.end(), ru.out) == s.rels.end())
             fail(p, RA_E_UNSUPPORTED, "SCC %d: rule output %s is not one of the SCC's relations", s.id,
                  p->rels[ru.out].name.c_str());
-    for (size_t i = 0; i < s.rels.size(); i++)
-        if (s.init[i]) full_to_delta(p, p->rels[s.rels[i]]);
+    p->loop_counter = 0;
+    if (!p->rs_dir.empty()) {
+        // restart (lie.cpp:300-330): deltas from the dump instead of full -> delta
+        for (int ri : s.rels) load_restart_delta(p, p->rels[ri]);
+    } else {
+        for (size_t i = 0; i < s.rels.size(); i++)
+            if (s.init[i]) full_to_delta(p, p->rels[s.rels[i]]);
+    }
     if (run_scc_dense(p, s)) {
-        for (int ri : s.rels) delta_to_full(p->rels[ri]);
+        p->pending_merge = s.rels;
         return;
     }
     {
         DevScc d;
         if (build_dev_scc(p, s, d)) {
             run_scc_device(p, s, d);
-            for (int ri : s.rels) delta_to_full(p->rels[ri]);
+            p->pending_merge = s.rels;
             return;
         }
     }
@@ -1737,9 +1907,10 @@ void run_scc(ra_program* p, Scc& s)
         }
         hist.push_back(d);
         hist.push_back(f);
+        checkpoint_batch(p, s, !s.fixpoint || d == 0, host_counts(p));
         if (!s.fixpoint || d == 0) break;
     }
-    for (int ri : s.rels) delta_to_full(p->rels[ri]);
+    p->pending_merge = s.rels;
     p->history.push_back((uint64_t)s.id);
     p->history.push_back(hist.size() / 2);
     p->history.insert(p->history.end(), hist.begin(), hist.end());
@@ -1794,6 +1965,7 @@ void reset_state(ra_program* p)
     }
     for (Scc& s : p->sccs) s.done = false;
     p->history.clear();
+    p->pending_merge.clear();
     p->iter_us.clear();
     p->inst_hist.clear();
     p->inst_hist_ok = true;
@@ -1867,6 +2039,8 @@ void begin_run(ra_program* p)
     }
     p->running = true;
     p->fixpoint_ms_acc = 0;
+    p->executed_ids = p->rs_skip;
+    if (p->cp_every) mkdir(p->cp_dir.c_str(), S_IRWXU | S_IRWXG | S_IROTH | S_IXOTH);
 }
 
 // LIE::one_runnable_tasks (src/lie/lie.cpp:27-60): first SCC, in add order, that
@@ -1885,6 +2059,7 @@ int next_runnable(ra_program* p)
 
 void finish_run(ra_program* p)
 {
+    merge_pending(p);
     CK(cudaStreamSynchronize(p->stream));
     double dms = 0;
     for (auto& e : p->dedup_events) {
@@ -1915,6 +2090,11 @@ int step(ra_program* p)
 {
     if (!p->running) begin_run(p);
     int next = next_runnable(p);
+    // a restart does not run the SCCs its dump lists as executed (lie.cpp:276-287)
+    while (next >= 0 && std::find(p->rs_skip.begin(), p->rs_skip.end(), p->sccs[next].id) != p->rs_skip.end()) {
+        p->sccs[next].done = true;
+        next = next_runnable(p);
+    }
     if (next < 0) {
         finish_run(p);
         return -1;
@@ -2303,6 +2483,34 @@ int ra_program_iteration_times(ra_program* p, double* out_us, uint64_t cap, uint
     return guard(p, [&] {
         if (len) *len = p->iter_us.size();
         if (out_us) std::memcpy(out_us, p->iter_us.data(), std::min<u64>(cap, p->iter_us.size()) * 8);
+    });
+}
+
+int ra_program_set_checkpoint(ra_program* p, const char* output_dir, uint32_t every_batches, int separate_files)
+{
+    return guard(p, [&] {
+        if (p->running) fail(p, RA_E_STATE, "set_checkpoint during a run");
+        if (every_batches && (!output_dir || !*output_dir)) fail(p, RA_E_BADARG, "checkpoint directory missing");
+        p->cp_every = every_batches;
+        p->cp_dir = every_batches ? std::string(output_dir) : std::string();
+        p->cp_separate = separate_files != 0;
+    });
+}
+
+int ra_program_set_restart(ra_program* p, const char* dump_dir, int separate_files)
+{
+    return guard(p, [&] {
+        if (p->running) fail(p, RA_E_STATE, "set_restart during a run");
+        p->rs_skip.clear();
+        p->rs_dir.clear();
+        if (!dump_dir || !*dump_dir) return;   // restart off
+        std::string dir(dump_dir);
+        while (dir.size() > 1 && dir.back() == '/') dir.pop_back();
+        p->rs_dir = dir;
+        p->rs_separate = separate_files != 0;
+        std::ifstream meta(dir + "/scc_metadata");
+        int id;
+        while (meta >> id) p->rs_skip.push_back(id);
     });
 }
 

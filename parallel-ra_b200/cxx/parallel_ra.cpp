@@ -119,8 +119,11 @@ bool LIE::execute()
     if (const char* e = getenv("RA_ID_ORDER"))
         RA_CK(prog, ra_program_set_id_order(prog, strcmp(e, "reference") == 0 ? RA_IDS_REFERENCE : RA_IDS_EMISSION));
 
-    if (enable_io || restart_flag)
-        fprintf(stderr, "parallel-RA (B200): checkpoint dumps and restart are not implemented; running without them\n");
+    /* checkpoint dumps (lie.cpp:154-193, 356-420) and restart (lie.cpp:260-330) */
+    RA_CK(prog, ra_program_set_checkpoint(prog, enable_io ? output_dir.c_str() : "",
+                                          enable_io && cp_iteration > 0 ? (uint32_t)cp_iteration : 0,
+                                          separate_io ? 1 : 0));
+    RA_CK(prog, ra_program_set_restart(prog, restart_flag ? restart_dir_name.c_str() : "", separate_io ? 1 : 0));
 
     std::map<relation*, int> handle;
     for (relation* r : lie_relations) {
@@ -130,7 +133,11 @@ bool LIE::execute()
                                        r->get_initailization_type() == DELTA ? RA_DELTA : RA_FULL, &h));
         r->bind(prog, h);
         handle[r] = h;
-        RA_CK(prog, ra_relation_load_file(prog, h, r->get_filename().c_str()));
+        /* relation::initialize_relation (balanced_hash_relation.cpp:744-756): a restart with
+         * per-rank files reads <file>_<rank> */
+        std::string file = r->get_filename();
+        if (restart_flag && separate_io) file += "_0";
+        RA_CK(prog, ra_relation_load_file(prog, h, file.c_str()));
     }
     auto rel = [&](relation* r) {
         auto it = handle.find(r);

@@ -35,6 +35,7 @@ EXPORTS = (
     "ra_relation_counts", "ra_relation_dump_full", "ra_rows_distinct_noalloc", "ra_status_string", "ra_last_error",
     "ra_program_set_instances", "ra_program_instance_history", "ra_relation_instance_summary",
     "ra_program_get_tuning", "ra_program_set_tuning", "ra_program_release",
+    "ra_program_set_checkpoint", "ra_program_set_restart",
 )
 
 
@@ -102,6 +103,8 @@ def lib():
         L.ra_program_run_next_scc.argtypes = [P, i32p]
         L.ra_program_reset.argtypes = [P]
         L.ra_program_release.argtypes = [P]
+        L.ra_program_set_checkpoint.argtypes = [P, C.c_char_p, C.c_uint32, C.c_int]
+        L.ra_program_set_restart.argtypes = [P, C.c_char_p, C.c_int]
         L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
         L.ra_program_iteration_times.argtypes = [P, C.POINTER(C.c_double), C.c_uint64, u64p]
@@ -224,6 +227,16 @@ class Program:
         if batch_size is not None:
             self.set_batch_size(batch_size)
         self._ck(self._L.ra_program_execute(self._p), "execute")
+
+    def set_checkpoint(self, output_dir: str, every_batches: int, separate_files: bool = False):
+        """Write the reference's checkpoint dumps every ``every_batches`` batches (0: off)."""
+        self._ck(self._L.ra_program_set_checkpoint(self._p, output_dir.encode(), every_batches,
+                                                   1 if separate_files else 0), "set_checkpoint")
+
+    def set_restart(self, dump_dir: str | None, separate_files: bool = False):
+        """Resume from a checkpoint dump directory (None: no restart)."""
+        self._ck(self._L.ra_program_set_restart(self._p, (dump_dir or "").encode(), 1 if separate_files else 0),
+                 "set_restart")
 
     def release(self):
         """Free the device buffers kept between runs (ends the last run)."""
