@@ -153,6 +153,18 @@ int ra_program_set_checkpoint(ra_program* p, const char* output_dir, uint32_t ev
  * The relations' full versions come from their own files (the dump's
  * <name>_full), as the program loads them.  dump_dir NULL or "" = no restart. */
 int ra_program_set_restart(ra_program* p, const char* dump_dir, int separate_files);
+/* Cap on the device memory the program may hold (0 = none): an allocation past
+ * it fails the run with RA_E_OOM, leaving the program reusable -- how a server
+ * keeps a program inside its share of the device, and how tests inject an
+ * out-of-memory failure from the host.  No reference counterpart. */
+int ra_program_set_memory_cap(ra_program* p, uint64_t bytes);
+/* Failure-path self-test of the device-side bounded waits: runs the engine's
+ * look-back wait on device `device` against a predecessor that never
+ * publishes, with a limit of max_polls polls (1 .. the engine's own limit).
+ * Returns RA_E_TIMEOUT when the wait gave up and reported it, as every engine
+ * wait does instead of spinning forever; the context stays usable.  No
+ * reference counterpart (the reference has no device waits). */
+int ra_selftest_bounded_wait(int device, uint64_t max_polls);
 /* Read / replace the program's tuning (RA_E_BADARG outside the ranges above;
  * RA_E_STATE during a run). */
 int ra_program_get_tuning(ra_program* p, ra_tuning* out);

@@ -145,6 +145,7 @@ struct ra_program {
     ra_stats stats{};
     std::unordered_map<void*, u64> alloc_bytes;   // live device allocations
     u64 live_bytes = 0;
+    u64 alloc_cap = 0;            // most device bytes the program may hold (0: no cap)
     // scratch
     u64* cand = nullptr;
     u64 cand_cap = 0;
@@ -238,6 +239,10 @@ void dev_alloc(ra_program* p, T** ptr, u64 count)
 {
     void* q = nullptr;
     if (count == 0) count = 1;
+    if (p->alloc_cap && p->live_bytes + count * sizeof(T) > p->alloc_cap)
+        fail(p, RA_E_OOM, "device-memory cap of %llu bytes reached (%llu held, %llu more asked)",
+             (unsigned long long)p->alloc_cap, (unsigned long long)p->live_bytes,
+             (unsigned long long)(count * sizeof(T)));
     CK(cudaMallocAsync(&q, count * sizeof(T), p->stream));
     *ptr = (T*)q;
     p->alloc_bytes[q] = count * sizeof(T);
@@ -2339,6 +2344,13 @@ int ra_relation_load_file(ra_program* p, int rel, const char* path)
         // parallel_io.cpp:180 asserts arity + 1 == col_count
         if (cols != r.arity + 1)
             fail(p, RA_E_IO, "%s: %llu columns, relation %s needs %u", meta.c_str(), cols, r.name.c_str(), r.arity + 1);
+        if (rows) {
+            struct stat st {};
+            if (stat(path, &st) != 0) fail(p, RA_E_IO, "cannot open %s", path);
+            if (rows > (unsigned long long)st.st_size / (8 * cols))
+                fail(p, RA_E_IO, "%s: %llu rows of %llu columns announced, the file holds %lld bytes", meta.c_str(),
+                     rows, cols, (long long)st.st_size);
+        }
         std::vector<uint64_t> buf((size_t)(rows * cols));
         if (rows) {
             FILE* d = fopen(path, "rb");
@@ -2434,8 +2446,7 @@ static int end_failed_run(ra_program* p, int st)
     if (p->stream) cudaStreamSynchronize(p->stream);
     cudaGetLastError();   // clear a non-sticky error (allocation failure) left by the run
     for (Scc& sc : p->sccs) drop_graph(sc);
-    p->running = false;
-    p->executed = false;
+    reset_state(p);       // every SCC runs again next time; counters, history and seen sets start over
     return st;
 }
 
@@ -2484,6 +2495,33 @@ int ra_program_iteration_times(ra_program* p, double* out_us, uint64_t cap, uint
         if (len) *len = p->iter_us.size();
         if (out_us) std::memcpy(out_us, p->iter_us.data(), std::min<u64>(cap, p->iter_us.size()) * 8);
     });
+}
+
+int ra_program_set_memory_cap(ra_program* p, uint64_t bytes)
+{
+    return guard(p, [&] { p->alloc_cap = bytes; });
+}
+
+int ra_selftest_bounded_wait(int device, uint64_t max_polls)
+{
+    if (cudaSetDevice(device) != cudaSuccess) return RA_E_CUDA;
+    if (max_polls == 0 || max_polls > kSpinLimit) return RA_E_BADARG;
+    void* mem = nullptr;
+    if (cudaMalloc(&mem, 4 * sizeof(u64)) != cudaSuccess) return RA_E_OOM;
+    u64* status = (u64*)mem;
+    u32* flags = (u32*)(status + 2);
+    int st = RA_OK;
+    if (cudaMemset(mem, 0, 4 * sizeof(u64)) != cudaSuccess) st = RA_E_CUDA;
+    if (st == RA_OK) {
+        lookback_selftest_kernel<<<1, 32>>>(status, flags, max_polls);
+        u32 hf = 0;
+        if (cudaGetLastError() != cudaSuccess || cudaMemcpy(&hf, flags, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = RA_E_CUDA;
+        else if (hf & kFlagTimeout)
+            st = RA_E_TIMEOUT;
+    }
+    cudaFree(mem);
+    return st;
 }
 
 int ra_program_set_checkpoint(ra_program* p, const char* output_dir, uint32_t every_batches, int separate_files)

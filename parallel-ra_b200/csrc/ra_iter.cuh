@@ -103,7 +103,9 @@ __device__ __forceinline__ const u64* rows_ptr(const IterCtl* c, const RowsRef& 
 constexpr u64 kStAgg = 1, kStIncl = 2;
 constexpr int kValBits = 38;
 constexpr u64 kValMask = (1ull << kValBits) - 1;
-constexpr u64 kSpinLimit = 1ull << 24;
+// polls before a look-back wait gives up (about a second of L2 round trips); a
+// predecessor tile is always resident and running, so a legitimate wait is far shorter
+constexpr u64 kSpinLimit = 1ull << 22;
 
 __device__ __forceinline__ u64 st_pack(u32 tag, u64 flag, u64 v)
 {
@@ -123,7 +125,7 @@ __device__ __forceinline__ u64 st_read(const u64* p) { return *((volatile const 
 
 // Exclusive prefix of tile `tile`'s aggregate `agg` over all earlier tiles.
 // Called by one thread.  Bounded: gives up after kSpinLimit polls (flag set).
-__device__ u64 lookback_one(u64* status, u32 tile, u64 agg, u32 tag, u32* flags)
+__device__ u64 lookback_one(u64* status, u32 tile, u64 agg, u32 tag, u32* flags, u64 limit = kSpinLimit)
 {
     if (tile == 0) {
         st_publish(&status[0], st_pack(tag, kStIncl, agg));
@@ -136,7 +138,7 @@ __device__ u64 lookback_one(u64* status, u32 tile, u64 agg, u32 tag, u32* flags)
     while (t >= 0) {
         u64 s = st_read(&status[t]);
         if (st_tag(s) != (tag & 0xffffffu) || st_flag(s) == 0) {
-            if (++spins > kSpinLimit) {
+            if (++spins > limit) {
                 atomicOr(flags, kFlagTimeout);
                 break;
             }
@@ -194,6 +196,13 @@ __device__ u64 lookback_warp(u64* status, u32 tile, u64 agg, u32 tag, u32* flags
     }
     if (lane == 0) st_publish(&status[tile], st_pack(tag, kStIncl, excl + agg));
     return excl;
+}
+
+// Failure-path self-test: tile 1 of a look-back whose tile 0 never publishes.
+// The wait must give up after `limit` polls and set kFlagTimeout.
+__global__ void lookback_selftest_kernel(u64* status, u32* flags, u64 limit)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) lookback_one(status, 1, 1, 7, flags, limit);
 }
 
 __device__ __forceinline__ u32 iter_tag(const IterCtl* c, int slot)

@@ -35,7 +35,8 @@ EXPORTS = (
     "ra_relation_counts", "ra_relation_dump_full", "ra_rows_distinct_noalloc", "ra_status_string", "ra_last_error",
     "ra_program_set_instances", "ra_program_instance_history", "ra_relation_instance_summary",
     "ra_program_get_tuning", "ra_program_set_tuning", "ra_program_release",
-    "ra_program_set_checkpoint", "ra_program_set_restart",
+    "ra_program_set_checkpoint", "ra_program_set_restart", "ra_program_set_memory_cap",
+    "ra_selftest_bounded_wait",
 )
 
 
@@ -105,6 +106,8 @@ def lib():
         L.ra_program_release.argtypes = [P]
         L.ra_program_set_checkpoint.argtypes = [P, C.c_char_p, C.c_uint32, C.c_int]
         L.ra_program_set_restart.argtypes = [P, C.c_char_p, C.c_int]
+        L.ra_program_set_memory_cap.argtypes = [P, C.c_uint64]
+        L.ra_selftest_bounded_wait.argtypes = [C.c_int, C.c_uint64]
         L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
         L.ra_program_iteration_times.argtypes = [P, C.POINTER(C.c_double), C.c_uint64, u64p]
@@ -238,6 +241,10 @@ class Program:
         self._ck(self._L.ra_program_set_restart(self._p, (dump_dir or "").encode(), 1 if separate_files else 0),
                  "set_restart")
 
+    def set_memory_cap(self, nbytes: int):
+        """Most device bytes the program may hold (0: no cap); beyond it a run fails with E_OOM."""
+        self._ck(self._L.ra_program_set_memory_cap(self._p, int(nbytes)), "set_memory_cap")
+
     def release(self):
         """Free the device buffers kept between runs (ends the last run)."""
         self._ck(self._L.ra_program_release(self._p), "release")
@@ -327,3 +334,8 @@ class Program:
                 raise KeyError(k)
             setattr(t, k, v)
         self._ck(self._L.ra_program_set_tuning(self._p, C.byref(t)), "set_tuning")
+
+
+def selftest_bounded_wait(device: int = 0, max_polls: int = 1 << 16) -> int:
+    """Status of the engine's bounded-wait self-test (E_TIMEOUT when the wait gave up as designed)."""
+    return lib().ra_selftest_bounded_wait(device, max_polls)

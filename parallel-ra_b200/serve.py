@@ -75,7 +75,7 @@ class WaveRecord:
 class Server:
     def __init__(self, device: int = 0, slots: int = 4, budget_bytes: float = 150e9,
                  wave_tuples: float | None = None, bytes_per_tuple: float | None = None,
-                 max_wave_requests: int = 8192, start: bool = True):
+                 max_wave_requests: int = 8192, program_cap_bytes: float | None = None, start: bool = True):
         self.device = device
         self.slots = slots
         self.budget = float(budget_bytes)
@@ -84,6 +84,10 @@ class Server:
         self.wave_tuples = float(wave_tuples or min(batch.WAVE_TUPLES, self.budget / (slots * b)))
         self.bpt = {"tc": b, "sg": b}               # device bytes per derived output tuple, learnt per kind
         self.max_wave_requests = max_wave_requests
+        # optional hard cap per program (ra_program_set_memory_cap): a wave past it fails fast with
+        # out of memory instead of growing into other workers' share; its retry alone is capped
+        # by the whole budget only
+        self.program_cap = int(program_cap_bytes) if program_cap_bytes else 0
         self.correction = {"tc": 1.0, "sg": 1.0}    # realised / estimated output tuples, learnt per kind
         self._queue: collections.deque[Request] = collections.deque()
         self._cv = threading.Condition()
@@ -197,6 +201,8 @@ class Server:
         rs = self._runners[w]
         if kind not in rs:
             rs[kind] = Runner(kind, self.device)
+            if self.program_cap:
+                rs[kind].prog.set_memory_cap(self.program_cap)
         return rs[kind]
 
     def _work(self, w: int) -> None:
@@ -277,6 +283,8 @@ class Server:
         try:
             return self._run_split(w, runner, reqs)
         finally:
+            if self.program_cap:
+                runner.prog.set_memory_cap(self.program_cap)
             with self._cv:
                 self._exclusive = None
                 self._cv.notify_all()
@@ -284,6 +292,8 @@ class Server:
     def _run_split(self, w: int, runner: Runner, reqs):
         for rr in self._runners[w].values():
             rr.prog.release()
+        if self.program_cap:
+            runner.prog.set_memory_cap(int(self.budget))
         try:
             return runner.run_wave([r.rows for r in reqs])
         except RAError as e:
