@@ -13,6 +13,7 @@
 namespace ra {
 
 typedef unsigned long long u64;
+typedef unsigned char u8;
 typedef unsigned int u32;
 
 constexpr u64 kEmpty = ~0ull;          // empty hash slot / filtered candidate

@@ -115,6 +115,11 @@ struct Relation {
     u64* csr_delta = nullptr;
     u64 csr_delta_version = ~0ull;
     u64 csr_delta_cap = 0;
+    // bitmap seen set (binary relations over small domains), kept between runs
+    u32* bm_seen = nullptr;
+    u32* bm_fresh = nullptr;
+    u8* bm_dirty = nullptr;
+    u64 bm_rows = 0;
     // newt staging for the running iteration
     u64 newt_n = 0;
 };
@@ -875,6 +880,7 @@ struct DevScc {
     std::vector<int> rel_of_slot;   // slot -> program relation index
     std::vector<uint32_t> tags;     // tag slot -> tag
     int passes[kMaxSccRels];
+    BitSeen bit[kMaxSccRels] = {};  // bitmap seen sets (bit[s].seen null: the hash set)
 };
 
 size_t ctl_header_bytes() { return offsetof(IterCtl, sort_hist); }
@@ -1028,8 +1034,11 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     u64 max_outer = 0;
     for (const DevRule& r : d.rules)
         max_outer = std::max(max_outer, r.in.slot >= 0 ? p->dcand_cap : r.in.static_n);
+    u64 bit_rows = 0;
+    for (int sl = 0; sl < d.plan.n_rels; sl++)
+        if (d.bit[sl].seen) bit_rows = std::max<u64>(bit_rows, d.bit[sl].n);
     u64 st_need = std::max<u64>({max_outer / kJRows + 2, p->dcand_cap / kSelTile + 2,
-                                 (p->stage_cap / kSortTile + 2) * kRadix});
+                                 (p->stage_cap / kSortTile + 2) * kRadix, bit_rows / kWarps + 2});
     if (st_need > p->status_cap) {
         dev_free(p, &p->status);
         dev_alloc(p, &p->status, st_need);
@@ -1056,7 +1065,7 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     for (int sl = 0; sl < pl.n_rels; sl++) {
         Relation& r = p->rels[d.rel_of_slot[sl]];
         pl.log_cap[sl] = r.cap;
-        pl.seen_limit[sl] = r.seen ? (u64)(p->tune.seen_load_max * (double)r.seen_cap) : 0;
+        pl.seen_limit[sl] = d.bit[sl].seen ? ~0ull : r.seen ? (u64)(p->tune.seen_load_max * (double)r.seen_cap) : 0;
     }
 }
 
@@ -1110,20 +1119,44 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         if (r.kind == kJoin)
             join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
                                                              p->bits, p->dcand, p->dcand_cap, out.seen,
-                                                             out.seen_cap, p->dloser, p->status, slot++);
+                                                             out.seen_cap, p->dloser, p->status, slot++,
+                                                             d.bit[r.out_slot]);
         else
             copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
                                                                  p->dcand, p->dcand_cap, out.seen, out.seen_cap,
-                                                                 p->dloser);
+                                                                 p->dloser, d.bit[r.out_slot]);
         launches++;
     }
+    // the selects: one per hash-set rule; one per bitmap relation (at its first rule)
+    auto selects_rule = [&](int q) {
+        const int sl = d.rules[q].out_slot;
+        return !d.bit[sl].seen || d.rm.rules_in[sl][0] == q;
+    };
+    int last_select = -1;
+    for (int q = 0; q < pl.n_rules; q++)
+        if (selects_rule(q)) last_select = q;
     for (int q = 0; q < pl.n_rules; q++) {
+        if (!selects_rule(q)) continue;
         const DevRule& r = d.rules[q];
         Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
         PhaseTimer pt(p, 3);
+        if (d.bit[r.out_slot].seen) {
+            BitSelectArgs b{};
+            b.rel = r.out_slot;
+            b.first_rule = q;
+            b.last = q == last_select ? 1 : 0;
+            b.dst_keys = out.keys;
+            b.dst_ids = out.ids;
+            b.bs = d.bit[r.out_slot];
+            b.bits = p->bits;
+            bitmap_select_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, b, p->status, slot++, p->dhist,
+                                                                 cond, use_cond);
+            launches++;
+            continue;
+        }
         SelectArgs a{};
         a.rule = q;
-        a.last = (!ref && q == pl.n_rules - 1) ? 1 : 0;
+        a.last = (!ref && q == last_select) ? 1 : 0;
         a.to_log = ref ? 0 : 1;
         a.dst_keys = ref ? p->stage_k[r.out_slot] : out.keys;
         a.dst_ids = ref ? p->stage_v[r.out_slot] : out.ids;
@@ -1204,6 +1237,7 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
     put(inst, sizeof inst);
     put(&p->n_inst, sizeof p->n_inst);
     put(&p->tune, sizeof p->tune);
+    put(d.bit, sizeof d.bit);
     put(&p->inst_rows_cap, sizeof p->inst_rows_cap);
     return sig;
 }
@@ -1333,6 +1367,41 @@ void load_restart_delta(ra_program* p, Relation& r)
     r.delta_version = fresh_stamp();
 }
 
+// Does output relation r of a device-driven SCC take a bitmap seen set?  Binary,
+// values below 65,536, default id order, no instances, bit matrices within the
+// tuned budget of the dense representations.
+bool bitmap_ok(ra_program* p, const Relation& r)
+{
+    const u64 rows = p->max_value + 1, words = (rows + 31) / 32;
+    return r.arity == 2 && p->n_inst == 0 && p->id_order == RA_IDS_EMISSION && rows <= kDenseMaxN &&
+           p->tune.dense_max_bytes > 0 && 8.0 * (double)(rows * words) + (double)rows <= p->tune.dense_max_bytes;
+}
+
+// r's bitmap seen set holding its stored tuples, fresh bits and dirty rows cleared.
+BitSeen prepare_bitmap(ra_program* p, Relation& r)
+{
+    const u64 rows = p->max_value + 1, words = (rows + 31) / 32;
+    if (r.bm_rows != rows) {
+        dev_free(p, &r.bm_seen);
+        dev_free(p, &r.bm_fresh);
+        dev_free(p, &r.bm_dirty);
+        dev_alloc(p, &r.bm_seen, rows * words);
+        dev_alloc(p, &r.bm_fresh, rows * words);
+        dev_alloc(p, &r.bm_dirty, rows);
+        r.bm_rows = rows;
+    }
+    CK(cudaMemsetAsync(r.bm_seen, 0, rows * words * 4, p->stream));
+    CK(cudaMemsetAsync(r.bm_fresh, 0, rows * words * 4, p->stream));
+    CK(cudaMemsetAsync(r.bm_dirty, 0, rows, p->stream));
+    BitSeen b{r.bm_seen, r.bm_fresh, r.bm_dirty, (u32)words, (u32)rows};
+    const u64 n = r.full_n + r.delta_n;
+    if (n) {
+        bitmap_build_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(b, r.keys, n, p->bits);
+        LAUNCHED();
+    }
+    return b;
+}
+
 // A completed iteration of run_scc_device that closed a batch (a new history
 // entry): counts of the SCC's relations from the control block.
 void checkpoint_device_batch(ra_program* p, const Scc& s, const DevScc& d, u64& hist_seen)
@@ -1383,8 +1452,14 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
         if (!d.rm.n_rules_in[sl]) continue;
         Relation& r = p->rels[d.rel_of_slot[sl]];
         u64 base = r.full_n + r.delta_n;
-        build_seen(p, r, std::max<u64>(2 * base, 1u << 20));
-        h.seen_n[sl] = r.seen_n;
+        if (bitmap_ok(p, r)) {
+            d.bit[sl] = prepare_bitmap(p, r);
+            h.seen_n[sl] = base;
+        } else {
+            d.bit[sl] = BitSeen{};
+            build_seen(p, r, std::max<u64>(2 * base, 1u << 20));
+            h.seen_n[sl] = r.seen_n;
+        }
         ensure_log(p, r, base + std::max<u64>(base, 1u << 20));
     }
     refresh_refs(p, d);
@@ -1456,7 +1531,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             u64 total = 0;
             u64 incoming[kMaxSccRels] = {0};
             for (int q = 0; q < pl.n_rules; q++) {
-                total += h.cand_n[q];
+                if (!d.bit[pl.rule_out[q]].seen) total += h.cand_n[q];   // bitmap rules write no candidates
                 incoming[pl.rule_out[q]] += h.cand_n[q];
             }
             u64 stage_need = 0;
@@ -1468,9 +1543,9 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 r.delta_n = h.delta_n[sl];
                 const u64 stored = r.full_n + r.delta_n;
                 if (replay && stored + incoming[sl] > r.cap) ensure_log(p, r, stored + 2 * incoming[sl]);
-                const bool tight =
+                const bool tight = !d.bit[sl].seen &&
                     h.seen_n[sl] + 2 * incoming[sl] > (u64)(p->tune.seen_load_max * (double)r.seen_cap);
-                if ((h.flags & kFlagProbe) || tight) {
+                if (!d.bit[sl].seen && ((h.flags & kFlagProbe) || tight)) {
                     // rebuild from the stored tuples: every key older than the next (or replayed) iteration;
                     // at least twice the slots (a probe overflow means long clusters)
                     const u64 want = std::max<u64>((u64)(p->tune.seen_grow * (double)(stored + incoming[sl])),
@@ -1526,7 +1601,8 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
         Relation& r = p->rels[d.rel_of_slot[sl]];
         // compare with the counts at SCC start (a mid-SCC regrow refreshes r's counts)
         if (h.full_n[sl] != full0[sl] || h.delta_n[sl] != delta0[sl] || h.iteration) {
-            const bool ref = p->id_order == RA_IDS_REFERENCE;
+            // deltas come out sorted in reference id order and from a bitmap relation's select
+            const bool ref = p->id_order == RA_IDS_REFERENCE || d.bit[sl].seen;
             if (h.runs[sl]) {
                 // one run into an empty full keeps it sorted when that run was sorted: the SCC's
                 // initial delta, or a new delta in reference id order
@@ -1540,6 +1616,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             r.delta_version = fresh_stamp();
         }
         if (d.rm.n_rules_in[sl]) r.seen_n = h.seen_n[sl];
+        if (d.bit[sl].seen && r.seen) r.seen_dirty = true;   // its hash set missed this SCC's tuples
     }
     for (size_t t = 0; t < d.tags.size(); t++) intern_counter(p, d.tags[t]) = h.intern[t];
     p->epoch = h.epoch;
@@ -1951,6 +2028,10 @@ void free_relation_state(ra_program* p, Relation& r)
     dev_free(p, &r.vids);
     dev_free(p, &r.csr_full);
     dev_free(p, &r.csr_delta);
+    dev_free(p, &r.bm_seen);
+    dev_free(p, &r.bm_fresh);
+    dev_free(p, &r.bm_dirty);
+    r.bm_rows = 0;
     r.cap = r.seen_cap = r.seen_n = r.v_cap = r.csr_full_cap = r.csr_delta_cap = 0;
     r.v_version = r.csr_full_version = r.csr_delta_version = ~0ull;
     r.full_n = r.delta_n = r.newt_n = 0;

@@ -305,6 +305,46 @@ __device__ __forceinline__ LoserMarks loser_marks(const IterCtl* c, u32* mark)
 }
 
 // ---------------------------------------------------------------------------
+// Bitmap seen set of a binary relation over a small value domain (at most
+// 65,536 values): bit c1 of row c0 is set for every tuple (c0, c1) the relation
+// holds.  A claim is a plain read and, for a new tuple, one atomicOr on a word of
+// a table a fraction of the size of the hash set; `fresh` collects the
+// iteration's new tuples and `dirty[c0]` marks rows holding some, from which
+// bitmap_select_kernel emits them in key order.  No candidate stream and no
+// loser marks: the set of new tuples is the same as the hash-set path's, and
+// their order (sorted) does not depend on which duplicate claimed first.
+// ---------------------------------------------------------------------------
+struct BitSeen {
+    u32* seen;      // null: the relation uses its hash seen set
+    u32* fresh;
+    u8* dirty;
+    u32 words;      // u32 words per row
+    u32 n;          // rows (values)
+};
+
+__device__ __forceinline__ void bit_claim(const BitSeen& b, u64 key, int bits)
+{
+    const u64 c0 = key >> bits, c1 = key & ((1ull << bits) - 1);
+    const u64 w = c0 * b.words + (c1 >> 5);
+    const u32 bit = 1u << (c1 & 31);
+    if (*((volatile u32*)&b.seen[w]) & bit) return;   // known: no atomic
+    if (atomicOr(&b.seen[w], bit) & bit) return;      // a duplicate claimed it first
+    atomicOr(&b.fresh[w], bit);
+    b.dirty[c0] = 1;
+}
+
+// Bits of a relation's stored tuples (its full and delta regions).
+__global__ void __launch_bounds__(kThreads) bitmap_build_kernel(BitSeen b, const u64* __restrict__ keys, u64 n,
+                                                                int bits)
+{
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads) {
+        const u64 k = keys[i];
+        const u64 c0 = k >> bits, c1 = k & ((1ull << bits) - 1);
+        atomicOr(&b.seen[c0 * b.words + (c1 >> 5)], 1u << (c1 & 31));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // join_fused: count + look-back scan + expansion + claim, one launch per rule
 // ---------------------------------------------------------------------------
 #ifndef RA_JOIN_ROWS_PER_THREAD
@@ -328,7 +368,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                                                               u64* __restrict__ cand, u64 cand_cap,
                                                               Slot* __restrict__ seen, u64 seen_cap,
                                                               u32* __restrict__ loser, u64* __restrict__ status,
-                                                              int tile_slot)
+                                                              int tile_slot, BitSeen bs)
 {
     __shared__ u64 s_ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
     __shared__ u64 s_start[kJRows];    // first inner row of each outer row
@@ -392,7 +432,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
             ctl->cand_n[rule] = prefix + agg;
             ctl->outer_rows += n;
         }
-        if (cbase + prefix + agg > cand_cap) {
+        if (!bs.seen && cbase + prefix + agg > cand_cap) {
             if (threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
         } else {
             // the tile's candidates: position prefix + j, j in [0, agg)
@@ -421,9 +461,15 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                     const u64 j = j0 + threadIdx.x + (u64)k * kThreads;
                     key[k] = valid[k] ? project(pj, s_key[rr[k]], ik[k], bits) : 0;
                     mine[k] = tag_base + prefix + j;
-                    if (valid[k]) cand[cbase + prefix + j] = key[k];
+                    if (valid[k] && !bs.seen) cand[cbase + prefix + j] = key[k];
                 }
-                claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
+                if (bs.seen) {
+#pragma unroll
+                    for (int k = 0; k < kClaimBatch; k++)
+                        if (valid[k]) bit_claim(bs, key[k], bits);
+                } else {
+                    claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
+                }
             }
         }
         __syncthreads();
@@ -435,14 +481,14 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
                                                               RowsRef in_ref, Projection pj, int bits, int pred,
                                                               u64* __restrict__ cand, u64 cand_cap,
                                                               Slot* __restrict__ seen, u64 seen_cap,
-                                                              u32* __restrict__ loser)
+                                                              u32* __restrict__ loser, BitSeen bs)
 {
     if (ctl->flags) return;
     const u64 c = rows_n(ctl, in_ref);
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = c;
     if (c == 0) return;
     const u64 cbase = stream_base(ctl, rule);
-    if (cbase + c > cand_cap) {
+    if (!bs.seen && cbase + c > cand_cap) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
         return;
     }
@@ -469,11 +515,17 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
                     keep = eval_pred(pred, a, b);
                 }
                 key[k] = keep ? project(pj, kk, 0, bits) : kEmpty;
-                out[p] = key[k];
+                if (!bs.seen) out[p] = key[k];
                 valid[k] = keep;
             }
         }
-        claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
+        if (bs.seen) {
+#pragma unroll
+            for (int k = 0; k < kClaimBatch; k++)
+                if (valid[k]) bit_claim(bs, key[k], bits);
+        } else {
+            claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
+        }
     }
     (void)plan;
 }
@@ -720,6 +772,137 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
 // ---------------------------------------------------------------------------
 constexpr int kSortIpt = 8;
 constexpr int kSortTile = kThreads * kSortIpt;
+
+// ---------------------------------------------------------------------------
+// bitmap_select: the new tuples of a bitmap relation (all rules into it at
+// once) into its log, in key order, one warp per row.  Takes part in the
+// iteration like select_kernel: the same capacity check before any write, the
+// same exit counter, the iteration end when it is the iteration's last launch.
+// ---------------------------------------------------------------------------
+struct BitSelectArgs {
+    int rel;          // output relation slot
+    int first_rule;   // the relation's first rule: credited with all its new tuples
+    int last;         // this launch ends the iteration
+    u64* dst_keys;
+    u64* dst_ids;
+    BitSeen bs;
+    int bits;         // packed column width
+};
+
+__global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
+                                                                 BitSelectArgs a, u64* __restrict__ status,
+                                                                 int tile_slot, u64* __restrict__ history,
+                                                                 cudaGraphConditionalHandle cond, int use_cond)
+{
+    __shared__ u64 sm[kWarps + 1];
+    __shared__ u64 s_cnt[kWarps];
+    __shared__ u32 s_tile;
+    __shared__ u64 s_prefix;
+    const int out = a.rel, tslot = plan.rule_tag[a.first_rule];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u64 rows = a.bs.n, W = a.bs.words;
+    const u64 ntiles = (rows + kWarps - 1) / kWarps;
+    bool active = ctl->flags == 0;
+    if (active) {
+        bool over = false;   // select_kernel's check: room for every candidate of the iteration
+        for (int s = 0; s < plan.n_rels; s++) {
+            u64 incoming = 0;
+            for (int q = 0; q < rm.n_rules_in[s]; q++) incoming += ctl->cand_n[rm.rules_in[s][q]];
+            if (incoming && ctl->full_n[s] + ctl->delta_n[s] + incoming > plan.log_cap[s]) over = true;
+        }
+        if (over) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
+            active = false;
+        }
+    }
+    if (active && blockIdx.x < ntiles) {
+        u64 dst_off = ctl->full_n[out] + ctl->delta_n[out], id_ctr = ctl->intern[tslot];
+        for (int q = 0; q < a.first_rule; q++)
+            if (plan.rule_tag[q] == tslot) id_ctr += ctl->win_n[q];
+        const u64 tag_word = plan.rel_tag_word[out];
+        const u32 tag = iter_tag(ctl, tile_slot);
+        u32* ctr = tile_counter(ctl, tile_slot);
+        for (;;) {
+            if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+            __syncthreads();
+            const u64 tile = s_tile;
+            __syncthreads();
+            if (tile >= ntiles) break;
+            const u64 row = tile * kWarps + warp;
+            const bool has = row < rows && a.bs.dirty[row];
+            u32* frow = a.bs.fresh + row * W;
+            u64 cnt = 0;
+            if (has)
+                for (u64 w = lane; w < W; w += 32) cnt += __popc(frow[w]);
+            for (int d = 16; d > 0; d >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+            if (lane == 0) s_cnt[warp] = cnt;
+            __syncthreads();
+            u64 agg;
+            const u64 ex = block_exclusive_scan(threadIdx.x < kWarps ? s_cnt[threadIdx.x] : 0, sm, &agg);
+            __syncthreads();
+            if (threadIdx.x < kWarps) s_cnt[threadIdx.x] = ex;   // row offsets inside the tile
+            if (threadIdx.x < 32) {
+                const u64 pre = lookback_warp(status, (u32)tile, agg, tag, &ctl->flags);
+                if (threadIdx.x == 0) s_prefix = pre;
+            }
+            __syncthreads();
+            if (has) {
+                u64 pos = s_prefix + s_cnt[warp];
+                for (u64 g = 0; g < W; g += 32) {
+                    const u32 word = (g + lane < W) ? frow[g + lane] : 0u;
+                    const u32 c = __popc(word);
+                    u32 incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const u32 t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    const u32 group = __shfl_sync(0xffffffffu, incl, 31);
+                    for (u32 t0 = 0; t0 < group; t0 += 32) {
+                        const u32 t = t0 + lane;
+                        u32 lo = 0, hi = 31;
+#pragma unroll
+                        for (int step = 0; step < 5; step++) {
+                            const u32 mid = (lo + hi) >> 1;
+                            if (__shfl_sync(0xffffffffu, incl, mid) > t) hi = mid;
+                            else lo = mid + 1;
+                        }
+                        const u32 wj = __shfl_sync(0xffffffffu, word, lo);
+                        const u32 before = __shfl_sync(0xffffffffu, incl - c, lo);
+                        if (t < group) {
+                            const u32 bit = __fns(wj, 0, (int)(t - before) + 1);
+                            const u64 c1 = (g + lo) * 32 + bit;
+                            const u64 at = pos + t;
+                            a.dst_keys[dst_off + at] = (row << a.bits) | c1;
+                            a.dst_ids[dst_off + at] = tag_word | (id_ctr + at);
+                        }
+                    }
+                    if (g + lane < W) frow[g + lane] = 0u;
+                    pos += group;
+                }
+                if (lane == 0) a.bs.dirty[row] = 0;
+            }
+            if (tile == ntiles - 1 && threadIdx.x == 0) {
+                ctl->win_n[a.first_rule] = s_prefix + agg;
+                for (int q = 0; q < rm.n_rules_in[out]; q++)
+                    if (rm.rules_in[out][q] != a.first_rule) ctl->win_n[rm.rules_in[out][q]] = 0;
+            }
+            __syncthreads();
+        }
+    }
+    const u32 parting = (u32)min((u64)gridDim.x, active ? ntiles : (u64)1);
+    if (blockIdx.x >= parting) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const u32 done = atomicAdd(&ctl->exit_ctr, 1u);
+        if (done == parting - 1) {
+            __threadfence();
+            ctl->exit_ctr = 0;
+            if (a.last) end_of_iteration(ctl, plan, rm, history, cond, use_cond);
+        }
+    }
+}
 
 struct SortPassArgs {
     int rel;                  // relation slot
