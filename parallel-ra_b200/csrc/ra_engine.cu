@@ -212,6 +212,13 @@ struct ra_program {
     std::vector<int> rs_skip;        // SCC ids a restart does not run again
     int loop_counter = 0;         // batches of the running SCC (LIE::execute's loop_counter)
     std::vector<int> pending_merge;  // relations of the last SCC whose delta still awaits full
+    // per-row tables of the instances' bit matrices (bitmap seen sets of batched runs)
+    u64* bmt_word = nullptr;
+    u32* bmt_base = nullptr;
+    u32* bmt_words = nullptr;
+    u32* bmt_inst = nullptr;
+    u64 bmt_rows = 0, bmt_total = 0;
+    std::vector<u64> bmt_bases;      // the instance bases the tables were built for
     bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
     bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
@@ -1149,6 +1156,11 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
             b.dst_ids = out.ids;
             b.bs = d.bit[r.out_slot];
             b.bits = p->bits;
+            if (p->n_inst) {
+                b.inst_new = p->dinst_new;
+                b.n_inst = p->n_inst;
+                b.inst_iter_cap = p->inst_rows_cap;
+            }
             bitmap_select_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, b, p->status, slot++, p->dhist,
                                                                  cond, use_cond);
             launches++;
@@ -1367,37 +1379,109 @@ void load_restart_delta(ra_program* p, Relation& r)
     r.delta_version = fresh_stamp();
 }
 
+// Words of the bit matrices a bitmap relation needs: one rows x rows matrix, or with
+// instances one n_i x n_i matrix per instance (0 when an instance is too wide).
+u64 bitmap_words(ra_program* p)
+{
+    const u64 rows = p->max_value + 1;
+    if (!p->n_inst) return rows <= kDenseMaxN ? rows * ((rows + 31) / 32) : 0;
+    u64 total = 0;
+    for (u32 i = 0; i < p->n_inst; i++) {
+        const u64 b = p->inst_base_h[i];
+        if (b >= rows) break;
+        const u64 e = std::min<u64>(p->inst_base_h[i + 1], rows), n = e - b;
+        if (n > kDenseMaxN) return 0;
+        total += n * ((n + 31) / 32);
+    }
+    return total;
+}
+
 // Does output relation r of a device-driven SCC take a bitmap seen set?  Binary,
-// values below 65,536, default id order, no instances, bit matrices within the
+// values (per instance) below 65,536, default id order, bit matrices within the
 // tuned budget of the dense representations.
 bool bitmap_ok(ra_program* p, const Relation& r)
 {
-    const u64 rows = p->max_value + 1, words = (rows + 31) / 32;
-    return r.arity == 2 && p->n_inst == 0 && p->id_order == RA_IDS_EMISSION && rows <= kDenseMaxN &&
-           p->tune.dense_max_bytes > 0 && 8.0 * (double)(rows * words) + (double)rows <= p->tune.dense_max_bytes;
+    if (r.arity != 2 || p->id_order != RA_IDS_EMISSION || p->tune.dense_max_bytes <= 0) return false;
+    const u64 words = bitmap_words(p);
+    return words && 8.0 * (double)words + (double)(p->max_value + 1) <= p->tune.dense_max_bytes;
+}
+
+// With instances: row v's word offset, base value, words per row and instance, for
+// every value of the union (built once per instance layout).
+void bitmap_tables(ra_program* p)
+{
+    const u64 rows = p->max_value + 1;
+    if (p->bmt_word && p->bmt_rows == rows && p->bmt_bases == p->inst_base_h) return;
+    std::vector<u64> word(rows, 0);
+    std::vector<u32> base(rows, 0), words(rows, 1), inst(rows, 0);
+    u64 off = 0;
+    for (u32 i = 0; i < p->n_inst; i++) {
+        const u64 b = p->inst_base_h[i];
+        if (b >= rows) break;
+        const u64 e = std::min<u64>(p->inst_base_h[i + 1], rows), n = e - b, w = (n + 31) / 32;
+        for (u64 v = b; v < e; v++) {
+            word[v] = off + (v - b) * w;
+            base[v] = (u32)b;
+            words[v] = (u32)w;
+            inst[v] = i;
+        }
+        off += n * w;
+    }
+    dev_free(p, &p->bmt_word);
+    dev_free(p, &p->bmt_base);
+    dev_free(p, &p->bmt_words);
+    dev_free(p, &p->bmt_inst);
+    dev_alloc(p, &p->bmt_word, rows);
+    dev_alloc(p, &p->bmt_base, rows);
+    dev_alloc(p, &p->bmt_words, rows);
+    dev_alloc(p, &p->bmt_inst, rows);
+    CK(cudaMemcpyAsync(p->bmt_word, word.data(), rows * 8, cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(p->bmt_base, base.data(), rows * 4, cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(p->bmt_words, words.data(), rows * 4, cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(p->bmt_inst, inst.data(), rows * 4, cudaMemcpyHostToDevice, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    p->bmt_rows = rows;
+    p->bmt_total = off;
+    p->bmt_bases = p->inst_base_h;
 }
 
 // r's bitmap seen set holding its stored tuples, fresh bits and dirty rows cleared.
 BitSeen prepare_bitmap(ra_program* p, Relation& r)
 {
-    const u64 rows = p->max_value + 1, words = (rows + 31) / 32;
-    if (r.bm_rows != rows) {
+    const u64 rows = p->max_value + 1;
+    if (p->n_inst) bitmap_tables(p);
+    const u64 words = p->n_inst ? p->bmt_total : rows * ((rows + 31) / 32);
+    if (r.bm_rows != words) {
         dev_free(p, &r.bm_seen);
         dev_free(p, &r.bm_fresh);
         dev_free(p, &r.bm_dirty);
-        dev_alloc(p, &r.bm_seen, rows * words);
-        dev_alloc(p, &r.bm_fresh, rows * words);
+        dev_alloc(p, &r.bm_seen, words);
+        dev_alloc(p, &r.bm_fresh, words);
         dev_alloc(p, &r.bm_dirty, rows);
-        r.bm_rows = rows;
+        r.bm_rows = words;   // capacity in words (rows <= words)
     }
-    CK(cudaMemsetAsync(r.bm_seen, 0, rows * words * 4, p->stream));
-    CK(cudaMemsetAsync(r.bm_fresh, 0, rows * words * 4, p->stream));
+    CK(cudaMemsetAsync(r.bm_seen, 0, words * 4, p->stream));
+    CK(cudaMemsetAsync(r.bm_fresh, 0, words * 4, p->stream));
     CK(cudaMemsetAsync(r.bm_dirty, 0, rows, p->stream));
-    BitSeen b{r.bm_seen, r.bm_fresh, r.bm_dirty, (u32)words, (u32)rows};
+    BitSeen b{};
+    b.seen = r.bm_seen;
+    b.fresh = r.bm_fresh;
+    b.dirty = r.bm_dirty;
+    b.words = (u32)((rows + 31) / 32);
+    b.n = (u32)rows;
+    if (p->n_inst) {
+        b.row_word = p->bmt_word;
+        b.row_base = p->bmt_base;
+        b.row_words = p->bmt_words;
+        b.row_inst = p->bmt_inst;
+    }
     const u64 n = r.full_n + r.delta_n;
     if (n) {
-        bitmap_build_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(b, r.keys, n, p->bits);
+        CK(cudaMemsetAsync(p->derr, 0, 4, p->stream));
+        bitmap_build_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(b, r.keys, n, p->bits, p->derr);
         LAUNCHED();
+        if (p->n_inst && (read_scalar(p, (const u64*)p->derr) & 0xffffffffull))
+            fail(p, RA_E_BADARG, "relation %s: a tuple's columns lie in different instances", r.name.c_str());
     }
     return b;
 }
@@ -1522,6 +1606,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             ctl_download(p);
         }
         if (h.flags & kFlagTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a device-side look-back wait gave up", s.id);
+        if (h.flags & kFlagRange) fail(p, RA_E_BADARG, "SCC %d: a derived tuple's columns lie in different instances", s.id);
         if (h.flags & (kFlagOverflow | kFlagProbe | kFlagGrow)) {
             // Overflow / probe: the iteration stopped before select wrote anything and its
             // claims are idempotent, so grow and replay it.  Grow: the iteration finished;
@@ -2102,6 +2187,12 @@ void release_buffers(ra_program* p)
     p->inst_rows_cap = 0;
     dev_free(p, &p->dhist);
     p->dhist_cap = 0;
+    dev_free(p, &p->bmt_word);
+    dev_free(p, &p->bmt_base);
+    dev_free(p, &p->bmt_words);
+    dev_free(p, &p->bmt_inst);
+    p->bmt_rows = 0;
+    p->bmt_bases.clear();
     for (Scc& sc : p->sccs) drop_graph(sc);
     CK(cudaStreamSynchronize(p->stream));
 }
@@ -2308,6 +2399,10 @@ int ra_program_destroy(ra_program* p)
     dev_free(p, &p->dhist);
     dev_free(p, &p->dinst_base);
     dev_free(p, &p->dinst_new);
+    dev_free(p, &p->bmt_word);
+    dev_free(p, &p->bmt_base);
+    dev_free(p, &p->bmt_words);
+    dev_free(p, &p->bmt_inst);
     for (Scc& sc : p->sccs) drop_graph(sc);
     for (auto& e : p->dedup_events) {
         cudaEventDestroy(e.first);

@@ -39,6 +39,7 @@ constexpr u32 kFlagOverflow = 1u;   // a buffer is too small: replay the iterati
 constexpr u32 kFlagTimeout = 2u;    // a bounded look-back wait gave up (fatal)
 constexpr u32 kFlagProbe = 4u;      // a seen-set probe gave up (table too full): grow, replay
 constexpr u32 kFlagGrow = 8u;       // iteration done; the seen set needs room before the next one
+constexpr u32 kFlagRange = 16u;     // a tuple whose columns lie in different instances (fatal)
 constexpr u64 kMaxProbe = 4096;
 
 struct IterCtl {
@@ -318,15 +319,40 @@ struct BitSeen {
     u32* seen;      // null: the relation uses its hash seen set
     u32* fresh;
     u8* dirty;
-    u32 words;      // u32 words per row
+    u32 words;      // u32 words per row (one matrix: no instances)
     u32 n;          // rows (values)
+    // with instances, one matrix per instance: row v's first word, the base value and
+    // the words of its instance's rows, the instance itself (null without instances)
+    const u64* row_word;
+    const u32* row_base;
+    const u32* row_words;
+    const u32* row_inst;
 };
 
-__device__ __forceinline__ void bit_claim(const BitSeen& b, u64 key, int bits)
+__device__ __forceinline__ u64 bit_word(const BitSeen& b, u64 c0, u64 c1)
+{
+    return b.row_word ? b.row_word[c0] + ((c1 - b.row_base[c0]) >> 5) : c0 * b.words + (c1 >> 5);
+}
+__device__ __forceinline__ u32 bit_of(const BitSeen& b, u64 c0, u64 c1)
+{
+    return 1u << ((b.row_word ? c1 - b.row_base[c0] : c1) & 31);
+}
+
+// With instances, is (c0, c1) inside c0's instance matrix?
+__device__ __forceinline__ bool bit_in_range(const BitSeen& b, u64 c0, u64 c1)
+{
+    return !b.row_word || ((c1 - b.row_base[c0]) >> 5) < b.row_words[c0];
+}
+
+__device__ __forceinline__ void bit_claim(const BitSeen& b, u64 key, int bits, u32* flags)
 {
     const u64 c0 = key >> bits, c1 = key & ((1ull << bits) - 1);
-    const u64 w = c0 * b.words + (c1 >> 5);
-    const u32 bit = 1u << (c1 & 31);
+    if (!bit_in_range(b, c0, c1)) {
+        atomicOr(flags, kFlagRange);
+        return;
+    }
+    const u64 w = bit_word(b, c0, c1);
+    const u32 bit = bit_of(b, c0, c1);
     if (*((volatile u32*)&b.seen[w]) & bit) return;   // known: no atomic
     if (atomicOr(&b.seen[w], bit) & bit) return;      // a duplicate claimed it first
     atomicOr(&b.fresh[w], bit);
@@ -335,12 +361,16 @@ __device__ __forceinline__ void bit_claim(const BitSeen& b, u64 key, int bits)
 
 // Bits of a relation's stored tuples (its full and delta regions).
 __global__ void __launch_bounds__(kThreads) bitmap_build_kernel(BitSeen b, const u64* __restrict__ keys, u64 n,
-                                                                int bits)
+                                                                int bits, u32* __restrict__ err)
 {
     for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads) {
         const u64 k = keys[i];
         const u64 c0 = k >> bits, c1 = k & ((1ull << bits) - 1);
-        atomicOr(&b.seen[c0 * b.words + (c1 >> 5)], 1u << (c1 & 31));
+        if (!bit_in_range(b, c0, c1)) {
+            *err = 1u;
+            continue;
+        }
+        atomicOr(&b.seen[bit_word(b, c0, c1)], bit_of(b, c0, c1));
     }
 }
 
@@ -466,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                 if (bs.seen) {
 #pragma unroll
                     for (int k = 0; k < kClaimBatch; k++)
-                        if (valid[k]) bit_claim(bs, key[k], bits);
+                        if (valid[k]) bit_claim(bs, key[k], bits, &ctl->flags);
                 } else {
                     claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
                 }
@@ -522,7 +552,7 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
         if (bs.seen) {
 #pragma unroll
             for (int k = 0; k < kClaimBatch; k++)
-                if (valid[k]) bit_claim(bs, key[k], bits);
+                if (valid[k]) bit_claim(bs, key[k], bits, &ctl->flags);
         } else {
             claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
         }
@@ -787,6 +817,9 @@ struct BitSelectArgs {
     u64* dst_ids;
     BitSeen bs;
     int bits;         // packed column width
+    u64* inst_new;    // [iteration][instance] new tuples (with instances), else null
+    u32 n_inst;
+    u64 inst_iter_cap;
 };
 
 __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
@@ -800,11 +833,12 @@ __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __rest
     __shared__ u64 s_prefix;
     const int out = a.rel, tslot = plan.rule_tag[a.first_rule];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const u64 rows = a.bs.n, W = a.bs.words;
+    const u64 rows = a.bs.n;
     const u64 ntiles = (rows + kWarps - 1) / kWarps;
     bool active = ctl->flags == 0;
     if (active) {
-        bool over = false;   // select_kernel's check: room for every candidate of the iteration
+        // select_kernel's check: room for every candidate of the iteration
+        bool over = a.inst_new && ctl->iteration >= a.inst_iter_cap;
         for (int s = 0; s < plan.n_rels; s++) {
             u64 incoming = 0;
             for (int q = 0; q < rm.n_rules_in[s]; q++) incoming += ctl->cand_n[rm.rules_in[s][q]];
@@ -830,7 +864,9 @@ __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __rest
             if (tile >= ntiles) break;
             const u64 row = tile * kWarps + warp;
             const bool has = row < rows && a.bs.dirty[row];
-            u32* frow = a.bs.fresh + row * W;
+            const u64 W = has && a.bs.row_word ? a.bs.row_words[row] : a.bs.words;
+            const u64 vbase = has && a.bs.row_word ? a.bs.row_base[row] : 0;
+            u32* frow = a.bs.fresh + (has && a.bs.row_word ? a.bs.row_word[row] : row * W);
             u64 cnt = 0;
             if (has)
                 for (u64 w = lane; w < W; w += 32) cnt += __popc(frow[w]);
@@ -871,7 +907,7 @@ __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __rest
                         const u32 before = __shfl_sync(0xffffffffu, incl - c, lo);
                         if (t < group) {
                             const u32 bit = __fns(wj, 0, (int)(t - before) + 1);
-                            const u64 c1 = (g + lo) * 32 + bit;
+                            const u64 c1 = vbase + (g + lo) * 32 + bit;
                             const u64 at = pos + t;
                             a.dst_keys[dst_off + at] = (row << a.bits) | c1;
                             a.dst_ids[dst_off + at] = tag_word | (id_ctr + at);
@@ -880,7 +916,12 @@ __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __rest
                     if (g + lane < W) frow[g + lane] = 0u;
                     pos += group;
                 }
-                if (lane == 0) a.bs.dirty[row] = 0;
+                if (lane == 0) {
+                    a.bs.dirty[row] = 0;
+                    if (a.inst_new)
+                        atomicAdd((unsigned long long*)&a.inst_new[ctl->iteration * a.n_inst + a.bs.row_inst[row]],
+                                  (unsigned long long)(pos - s_prefix - s_cnt[warp]));
+                }
             }
             if (tile == ntiles - 1 && threadIdx.x == 0) {
                 ctl->win_n[a.first_rule] = s_prefix + agg;

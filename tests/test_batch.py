@@ -182,3 +182,15 @@ def test_plan_waves_respects_dense_bytes():
     cap = 2.5 * dense_bytes(1000)
     waves = plan_waves([1, 1, 1, 1], budget_tuples=1e9, spans=spans, max_dense_bytes=cap)
     assert waves == [[0, 1], [2], [3]]
+
+
+@pytest.mark.gpu
+def test_tuple_across_instances_is_rejected():
+    """An edge whose endpoints lie in different declared instances is a caller error:
+    the run fails with RA_E_BADARG (no silent result, no out-of-range access)."""
+    p = P.Program(0)
+    rels = P.programs.build_tc(p, np.array([[0, 1, 0], [1, 2, 1], [3, 7, 2], [6, 5, 3]], dtype=np.uint64))
+    p.set_instances([0, 5])
+    with pytest.raises(P.RAError) as e:
+        p.execute(1)
+    assert e.value.status == P.engine.E_BADARG
