@@ -102,6 +102,7 @@ typedef struct ra_stats {
      * device time of the row searches and of the emission of new tuples. */
     double dense_search_ms;
     double dense_emit_ms;
+    uint64_t bitmap_relations;  /* output relations of device-driven SCCs that used a bitmap seen set */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose

@@ -51,13 +51,22 @@ struct DenseArgs {
     u64* inst_level;             // [iteration][instance] new tuples, or null
     u64 level_cap;
     u64* inst_init;              // per instance: tuples of the initial delta
-    u64* counters;               // [0], [2..4] chunks taken (per kernel shape), [1] join candidates (S rows visited)
+    u64* counters;               // [0], [2..4] chunks taken (per kernel shape), [1] join candidates (S rows visited),
+                                 // [5] 1 + the first key found outside its instance, [6] its relation (1: R, 2: S)
     u32* flags;
 };
 
 __device__ __forceinline__ u32 dense_instance(const DenseArgs& a, u64 v)
 {
     return a.inst_base ? instance_of(a.inst_base, a.n_inst, v) : 0u;
+}
+
+// A key with a value outside its row's instance: flag the run, keep the first such key.
+__device__ __forceinline__ void dense_range_error(const DenseArgs& a, u64 key, u64 which)
+{
+    atomicOr(a.flags, kDenseFlagRange);
+    if (atomicCAS((unsigned long long*)&a.counters[5], 0ull, (unsigned long long)(key + 1)) == 0ull)
+        atomicExch((unsigned long long*)&a.counters[6], (unsigned long long)which);
 }
 
 // Bits of R's stored tuples: all of them into `known`, the delta region's also into `delta0`.
@@ -71,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) dense_load_kernel(DenseArgs a, const
         const DenseInst d = a.inst[inst];
         const u64 r = x - d.base, c = y - d.base;   // unsigned: values below the base wrap high
         if (r >= d.n || c >= d.n) {
-            atomicOr(a.flags, kDenseFlagRange);
+            dense_range_error(a, k, 1);
             continue;
         }
         const u64 w = d.word_off + r * d.words + (c >> 5);
@@ -96,7 +105,7 @@ __global__ void __launch_bounds__(kThreads) dense_local_kernel(DenseArgs a, u64 
         const u64 zl = z - d.base;
         if (zl >= d.n || y - d.base >= d.n) {
             a.s_local[j] = 0xffffffffu;
-            atomicOr(a.flags, kDenseFlagRange);
+            dense_range_error(a, k, 2);
         } else {
             a.s_local[j] = (u32)zl;
         }

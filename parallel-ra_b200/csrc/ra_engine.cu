@@ -119,7 +119,8 @@ struct Relation {
     u32* bm_seen = nullptr;
     u32* bm_fresh = nullptr;
     u8* bm_dirty = nullptr;
-    u64 bm_rows = 0;
+    u64 bm_words = 0;             // capacity of bm_seen / bm_fresh (u32 words)
+    u64 bm_rows = 0;              // capacity of bm_dirty (rows)
     // newt staging for the running iteration
     u64 newt_n = 0;
 };
@@ -303,6 +304,7 @@ void grow1(ra_program* p, u64** a, u64* cap, u64 n)
     if (n <= *cap) return;
     u64 nc = std::max<u64>(n + n / 2, 1024);
     dev_free(p, a);
+    *cap = 0;   // a failed allocation leaves no stale capacity behind
     dev_alloc(p, a, nc);
     *cap = nc;
 }
@@ -1038,9 +1040,12 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
             dev_alloc(p, &p->stage_k[sl], p->stage_cap);
             dev_alloc(p, &p->stage_v[sl], p->stage_cap);
         }
+    // outer rows of a join: a static input's rows, or an SCC relation's delta -- at most its
+    // log's capacity, and (hash-set outputs) at most the candidates of one iteration
     u64 max_outer = 0;
     for (const DevRule& r : d.rules)
-        max_outer = std::max(max_outer, r.in.slot >= 0 ? p->dcand_cap : r.in.static_n);
+        max_outer = std::max(max_outer, r.in.slot >= 0 ? std::max(p->dcand_cap, p->rels[d.rel_of_slot[r.in.slot]].cap)
+                                                       : r.in.static_n);
     u64 bit_rows = 0;
     for (int sl = 0; sl < d.plan.n_rels; sl++)
         if (d.bit[sl].seen) bit_rows = std::max<u64>(bit_rows, d.bit[sl].n);
@@ -1126,8 +1131,8 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         if (r.kind == kJoin)
             join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
                                                              p->bits, p->dcand, p->dcand_cap, out.seen,
-                                                             out.seen_cap, p->dloser, p->status, slot++,
-                                                             d.bit[r.out_slot]);
+                                                             out.seen_cap, p->dloser, p->status, p->status_cap,
+                                                             slot++, d.bit[r.out_slot]);
         else
             copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
                                                                  p->dcand, p->dcand_cap, out.seen, out.seen_cap,
@@ -1161,8 +1166,8 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
                 b.n_inst = p->n_inst;
                 b.inst_iter_cap = p->inst_rows_cap;
             }
-            bitmap_select_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, b, p->status, slot++, p->dhist,
-                                                                 cond, use_cond);
+            bitmap_select_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, b, p->status, p->status_cap,
+                                                                 slot++, p->dhist, cond, use_cond);
             launches++;
             continue;
         }
@@ -1251,6 +1256,7 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
     put(&p->tune, sizeof p->tune);
     put(d.bit, sizeof d.bit);
     put(&p->inst_rows_cap, sizeof p->inst_rows_cap);
+    put(&p->status_cap, sizeof p->status_cap);
     return sig;
 }
 
@@ -1431,6 +1437,8 @@ void bitmap_tables(ra_program* p)
     dev_free(p, &p->bmt_base);
     dev_free(p, &p->bmt_words);
     dev_free(p, &p->bmt_inst);
+    p->bmt_rows = 0;
+    p->bmt_bases.clear();
     dev_alloc(p, &p->bmt_word, rows);
     dev_alloc(p, &p->bmt_base, rows);
     dev_alloc(p, &p->bmt_words, rows);
@@ -1451,14 +1459,19 @@ BitSeen prepare_bitmap(ra_program* p, Relation& r)
     const u64 rows = p->max_value + 1;
     if (p->n_inst) bitmap_tables(p);
     const u64 words = p->n_inst ? p->bmt_total : rows * ((rows + 31) / 32);
-    if (r.bm_rows != words) {
+    if (r.bm_words < words) {
         dev_free(p, &r.bm_seen);
         dev_free(p, &r.bm_fresh);
-        dev_free(p, &r.bm_dirty);
+        r.bm_words = 0;
         dev_alloc(p, &r.bm_seen, words);
         dev_alloc(p, &r.bm_fresh, words);
+        r.bm_words = words;
+    }
+    if (r.bm_rows < rows) {
+        dev_free(p, &r.bm_dirty);
+        r.bm_rows = 0;
         dev_alloc(p, &r.bm_dirty, rows);
-        r.bm_rows = words;   // capacity in words (rows <= words)
+        r.bm_rows = rows;
     }
     CK(cudaMemsetAsync(r.bm_seen, 0, words * 4, p->stream));
     CK(cudaMemsetAsync(r.bm_fresh, 0, words * 4, p->stream));
@@ -1539,6 +1552,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
         if (bitmap_ok(p, r)) {
             d.bit[sl] = prepare_bitmap(p, r);
             h.seen_n[sl] = base;
+            p->stats.bitmap_relations++;
         } else {
             d.bit[sl] = BitSeen{};
             build_seen(p, r, std::max<u64>(2 * base, 1u << 20));
@@ -1607,6 +1621,8 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
         }
         if (h.flags & kFlagTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a device-side look-back wait gave up", s.id);
         if (h.flags & kFlagRange) fail(p, RA_E_BADARG, "SCC %d: a derived tuple's columns lie in different instances", s.id);
+        if (h.flags & kFlagStatus)
+            fail(p, RA_E_UNSUPPORTED, "SCC %d: a launch has more tiles than its look-back status array holds", s.id);
         if (h.flags & (kFlagOverflow | kFlagProbe | kFlagGrow)) {
             // Overflow / probe: the iteration stopped before select wrote anything and its
             // claims are idempotent, so grow and replay it.  Grow: the iteration finished;
@@ -1930,9 +1946,21 @@ bool run_scc_dense(ra_program* p, Scc& s)
         u32 fl = 0;
         CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
         CK(cudaStreamSynchronize(p->stream));
-        if (fl & kDenseFlagRange)
-            fail(p, RA_E_BADARG, "SCC %d: a value of %s or %s lies outside its instance's range", s.id,
-                 R.name.c_str(), S.name.c_str());
+        if (fl & kDenseFlagRange) {
+            u64 bad[2] = {0, 0};
+            CK(cudaMemcpyAsync(bad, B.counters + 5, 16, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+            const u64 key = bad[0] - 1, mask = (1ull << p->bits) - 1;
+            const u64 c0 = (key >> p->bits) & mask, c1 = key & mask;
+            // R's rows are keyed by column 1's instance, S's by column 0's
+            const u64 at = bad[1] == 1 ? c1 : c0;
+            u32 inst = 0;
+            while (p->n_inst && inst + 1 < p->n_inst && p->inst_base_h[inst + 1] <= at) inst++;
+            fail(p, RA_E_BADARG,
+                 "SCC %d: tuple (%llu, %llu) of %s has a value outside its instance %u (values %llu .. %llu)",
+                 s.id, (unsigned long long)c0, (unsigned long long)c1, bad[1] == 1 ? R.name.c_str() : S.name.c_str(),
+                 inst, (unsigned long long)hi[inst].base, (unsigned long long)(hi[inst].base + hi[inst].n - 1));
+        }
         if (!(fl & kDenseFlagLevels)) {
             level_cap = a.level_cap;
             break;
@@ -2116,7 +2144,7 @@ void free_relation_state(ra_program* p, Relation& r)
     dev_free(p, &r.bm_seen);
     dev_free(p, &r.bm_fresh);
     dev_free(p, &r.bm_dirty);
-    r.bm_rows = 0;
+    r.bm_rows = r.bm_words = 0;
     r.cap = r.seen_cap = r.seen_n = r.v_cap = r.csr_full_cap = r.csr_delta_cap = 0;
     r.v_version = r.csr_full_version = r.csr_delta_version = ~0ull;
     r.full_n = r.delta_n = r.newt_n = 0;
@@ -2608,8 +2636,9 @@ int ra_scc_depend(ra_program* p, int src_scc, int dst_scc)
 
 // A run that failed (out of device memory, a device wait that timed out, ...)
 // leaves the program reusable: an open stream capture is closed, queued work
-// drains, and the run ends -- the next execute starts from the loaded state
-// and ra_program_release can free what the failed run had allocated.
+// drains, every device buffer of the run is freed (a failure may have struck
+// between a buffer's release and its regrowth), and the run ends -- the next
+// execute starts from the loaded state.
 static int end_failed_run(ra_program* p, int st)
 {
     if (st == RA_OK || !p) return st;
@@ -2621,7 +2650,12 @@ static int end_failed_run(ra_program* p, int st)
     }
     if (p->stream) cudaStreamSynchronize(p->stream);
     cudaGetLastError();   // clear a non-sticky error (allocation failure) left by the run
-    for (Scc& sc : p->sccs) drop_graph(sc);
+    const std::string msg = p->err;
+    try {
+        release_buffers(p);   // also drops every SCC's graph
+    } catch (...) {
+    }
+    p->err = msg;
     reset_state(p);       // every SCC runs again next time; counters, history and seen sets start over
     return st;
 }

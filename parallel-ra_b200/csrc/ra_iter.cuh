@@ -40,6 +40,7 @@ constexpr u32 kFlagTimeout = 2u;    // a bounded look-back wait gave up (fatal)
 constexpr u32 kFlagProbe = 4u;      // a seen-set probe gave up (table too full): grow, replay
 constexpr u32 kFlagGrow = 8u;       // iteration done; the seen set needs room before the next one
 constexpr u32 kFlagRange = 16u;     // a tuple whose columns lie in different instances (fatal)
+constexpr u32 kFlagStatus = 32u;    // a launch has more tiles than the look-back status array (fatal)
 constexpr u64 kMaxProbe = 4096;
 
 struct IterCtl {
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                                                               u64* __restrict__ cand, u64 cand_cap,
                                                               Slot* __restrict__ seen, u64 seen_cap,
                                                               u32* __restrict__ loser, u64* __restrict__ status,
-                                                              int tile_slot, BitSeen bs)
+                                                              u64 status_cap, int tile_slot, BitSeen bs)
 {
     __shared__ u64 s_ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
     __shared__ u64 s_start[kJRows];    // first inner row of each outer row
@@ -414,6 +415,10 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
         return;
     }
     const u64 ntiles = (n + kJRows - 1) / kJRows;
+    if (ntiles > status_cap) {   // the host sizes status for the largest outer input: never taken
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagStatus);
+        return;
+    }
     if (blockIdx.x >= ntiles) return;
     const u64 cbase = stream_base(ctl, rule);
     const u64 tag_base = (ctl->epoch << 40) | cbase;
@@ -824,7 +829,7 @@ struct BitSelectArgs {
 
 __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
                                                                  BitSelectArgs a, u64* __restrict__ status,
-                                                                 int tile_slot, u64* __restrict__ history,
+                                                                 u64 status_cap, int tile_slot, u64* __restrict__ history,
                                                                  cudaGraphConditionalHandle cond, int use_cond)
 {
     __shared__ u64 sm[kWarps + 1];
@@ -836,6 +841,10 @@ __global__ void __launch_bounds__(kThreads) bitmap_select_kernel(IterCtl* __rest
     const u64 rows = a.bs.n;
     const u64 ntiles = (rows + kWarps - 1) / kWarps;
     bool active = ctl->flags == 0;
+    if (active && ntiles > status_cap) {   // never taken: status is sized for the rows
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagStatus);
+        active = false;
+    }
     if (active) {
         // select_kernel's check: room for every candidate of the iteration
         bool over = a.inst_new && ctl->iteration >= a.inst_iter_cap;

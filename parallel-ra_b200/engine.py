@@ -54,7 +54,7 @@ class Stats(C.Structure):
         ("reserved", C.c_uint32), ("phase_ms", C.c_double * 6), ("graph_builds", C.c_uint64),
         ("graph_build_ms", C.c_double), ("regrows", C.c_uint64), ("device_bytes", C.c_uint64),
         ("device_bytes_peak", C.c_uint64), ("dense_sccs", C.c_uint64), ("dense_search_ms", C.c_double),
-        ("dense_emit_ms", C.c_double),
+        ("dense_emit_ms", C.c_double), ("bitmap_relations", C.c_uint64),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 

@@ -102,6 +102,7 @@ class Server:
         self._workers = [threading.Thread(target=self._work, args=(i,), daemon=True) for i in range(slots)]
         self._runners: list[dict] = [dict() for _ in range(slots)]
         self._errors: list[BaseException] = []
+        self.failed_waves: list[tuple] = []  # (worker, kind, request ids) of waves that raised
         if start:
             for t in self._workers:
                 t.start()
@@ -127,6 +128,7 @@ class Server:
                     raise TimeoutError(f"{len(self.completed)} of {expected} requests completed")
                 self._cv.wait(min(left, 0.5))
         if self._errors:
+            self.close()   # stop and join the workers before the failure propagates
             raise RuntimeError("a serving worker failed") from self._errors[0]
 
     def close(self) -> None:
@@ -206,6 +208,7 @@ class Server:
         return rs[kind]
 
     def _work(self, w: int) -> None:
+        current = None
         try:
             while True:
                 with self._cv:
@@ -217,6 +220,7 @@ class Server:
                         if job is None:
                             self._cv.wait(0.05)
                     kind, reqs, est = job
+                    current = (w, kind, [r.rid for r in reqs])
                     wid = self._wave_id
                     self._wave_id += 1
                 runner = self._runner(w, kind)
@@ -258,10 +262,13 @@ class Server:
                     self._used[w] = float(total_held)
                     self._busy[w] = False
                     self.completed.extend(reqs)
+                    current = None
                     self._cv.notify_all()
         except BaseException as e:  # surface worker failures to drain()
             with self._cv:
                 self._errors.append(e)
+                if current is not None:
+                    self.failed_waves.append(current)
                 self._cv.notify_all()
 
     def _retry_alone(self, w: int, runner: Runner, reqs):

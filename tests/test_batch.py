@@ -128,6 +128,27 @@ def test_sg_wave_matches_plain_and_oracle():
 
 
 @pytest.mark.gpu
+def test_sg_wave_with_large_deltas_matches_hash_path():
+    """Same generation over trees of up to 16,384 nodes: about 10^8 tuples, with
+    per-iteration deltas far above the 4M-row candidate buffer, through the
+    instances' bitmap seen sets; the wave equals the hash-set wave and plain runs."""
+    insts = [P.datagen.with_row_ids(P.datagen.random_tree(n, s)) for n, s in ((16384, 1), (8192, 3), (2000, 5))]
+    w = P.batch.Runner("sg")
+    got = w.run_wave(insts)
+    assert w.prog.stats().bitmap_relations >= 3
+    h = P.batch.Runner("sg")
+    h.prog.set_tuning(dense_max_bytes=0)
+    got_h = h.run_wave(insts)
+    assert h.prog.stats().bitmap_relations == 0
+    plain = P.batch.Runner("sg")
+    for i, rows in enumerate(insts):
+        assert got[i].key() == got_h[i].key() == plain.run_plain(rows).key(), i
+    assert max(max(d) for d in got[0].deltas if d) > 1 << 22
+    for r in (w, h, plain):
+        r.close()
+
+
+@pytest.mark.gpu
 def test_wave_in_reference_id_order():
     insts = small_instances(12, 9)
     got = P.batch.Runner("tc", id_order=P.engine.IDS_REFERENCE).run_wave(insts)

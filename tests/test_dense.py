@@ -93,3 +93,25 @@ def test_sg_and_reference_ids_keep_the_hash_path():
     P.programs.build_tc(q, er(300, 450, 8))
     q.execute(1)
     assert q.stats().dense_sccs == 0
+
+
+def test_bitmap_join_with_deltas_beyond_the_candidate_buffer():
+    """The TC join SCC on the device path with a bitmap seen set on T (the dense
+    evaluator declined: the budget lies between the bitmap's and the evaluator's
+    needs).  Its deltas reach tens of millions of tuples, far above the 4M-row
+    candidate buffer, and feed the next iteration's join, whose look-back status
+    array is sized by T's log.  History and tuples equal the dense evaluator's."""
+    n = 16384
+    rows = er(n, 2 * n, 12)
+    pb = P.Program(0)
+    pb.set_tuning(dense_max_bytes=8 * n * (n // 32) + 4 * n)
+    rb = P.programs.build_tc(pb, rows)
+    pb.execute(1)
+    st = pb.stats()
+    assert st.dense_sccs == 0 and st.bitmap_relations >= 1
+    pd, rd = run(rows, True)
+    assert pd.stats().dense_sccs == 1
+    hb = pb.history()
+    assert hb == pd.history()
+    assert max(d for _, pairs in hb for d, _ in pairs) > 1 << 22
+    assert np.array_equal(pb.dump_full(rb["T"])[:, :-1], pd.dump_full(rd["T"])[:, :-1])
