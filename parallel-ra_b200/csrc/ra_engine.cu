@@ -1404,34 +1404,31 @@ u64 bitmap_words(ra_program* p)
 
 // Does output relation r of a device-driven SCC take a bitmap seen set?  Binary,
 // values (per instance) below 65,536, default id order, bit matrices within the
-// tuned budget of the dense representations.
-bool bitmap_ok(ra_program* p, const Relation& r)
+// tuned budget of the dense representations, and a fixpoint SCC: a bitmap costs
+// clearing and scanning rows x rows bits, paid back only by the many iterations and
+// tuples of a recursive SCC (one pass of a copy or join costs its candidates only).
+bool bitmap_ok(ra_program* p, const Scc& s, const Relation& r)
 {
-    if (r.arity != 2 || p->id_order != RA_IDS_EMISSION || p->tune.dense_max_bytes <= 0) return false;
+    if (!s.fixpoint || r.arity != 2 || p->id_order != RA_IDS_EMISSION || p->tune.dense_max_bytes <= 0) return false;
     const u64 words = bitmap_words(p);
     return words && 8.0 * (double)words + (double)(p->max_value + 1) <= p->tune.dense_max_bytes;
 }
 
 // With instances: row v's word offset, base value, words per row and instance, for
-// every value of the union (built once per instance layout).
+// every value of the union (built on the device once per instance layout; the host
+// computes only each instance's first word).
 void bitmap_tables(ra_program* p)
 {
     const u64 rows = p->max_value + 1;
     if (p->bmt_word && p->bmt_rows == rows && p->bmt_bases == p->inst_base_h) return;
-    std::vector<u64> word(rows, 0);
-    std::vector<u32> base(rows, 0), words(rows, 1), inst(rows, 0);
+    std::vector<u64> first(p->n_inst, 0);
     u64 off = 0;
     for (u32 i = 0; i < p->n_inst; i++) {
+        first[i] = off;
         const u64 b = p->inst_base_h[i];
-        if (b >= rows) break;
-        const u64 e = std::min<u64>(p->inst_base_h[i + 1], rows), n = e - b, w = (n + 31) / 32;
-        for (u64 v = b; v < e; v++) {
-            word[v] = off + (v - b) * w;
-            base[v] = (u32)b;
-            words[v] = (u32)w;
-            inst[v] = i;
-        }
-        off += n * w;
+        if (b >= rows) continue;
+        const u64 n = std::min<u64>(p->inst_base_h[i + 1], rows) - b;
+        off += n * ((n + 31) / 32);
     }
     dev_free(p, &p->bmt_word);
     dev_free(p, &p->bmt_base);
@@ -1443,10 +1440,14 @@ void bitmap_tables(ra_program* p)
     dev_alloc(p, &p->bmt_base, rows);
     dev_alloc(p, &p->bmt_words, rows);
     dev_alloc(p, &p->bmt_inst, rows);
-    CK(cudaMemcpyAsync(p->bmt_word, word.data(), rows * 8, cudaMemcpyHostToDevice, p->stream));
-    CK(cudaMemcpyAsync(p->bmt_base, base.data(), rows * 4, cudaMemcpyHostToDevice, p->stream));
-    CK(cudaMemcpyAsync(p->bmt_words, words.data(), rows * 4, cudaMemcpyHostToDevice, p->stream));
-    CK(cudaMemcpyAsync(p->bmt_inst, inst.data(), rows * 4, cudaMemcpyHostToDevice, p->stream));
+    u64* dfirst;
+    dev_alloc(p, &dfirst, p->n_inst);
+    CK(cudaMemcpyAsync(dfirst, first.data(), p->n_inst * 8, cudaMemcpyHostToDevice, p->stream));
+    bitmap_tables_kernel<<<grid_for(rows), kThreads, 0, p->stream>>>(p->dinst_base, p->n_inst, dfirst, rows,
+                                                                     p->bmt_word, p->bmt_base, p->bmt_words,
+                                                                     p->bmt_inst);
+    LAUNCHED();
+    dev_free(p, &dfirst);
     CK(cudaStreamSynchronize(p->stream));
     p->bmt_rows = rows;
     p->bmt_total = off;
@@ -1549,7 +1550,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
         if (!d.rm.n_rules_in[sl]) continue;
         Relation& r = p->rels[d.rel_of_slot[sl]];
         u64 base = r.full_n + r.delta_n;
-        if (bitmap_ok(p, r)) {
+        if (bitmap_ok(p, s, r)) {
             d.bit[sl] = prepare_bitmap(p, r);
             h.seen_n[sl] = base;
             p->stats.bitmap_relations++;

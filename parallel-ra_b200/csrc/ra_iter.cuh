@@ -674,6 +674,25 @@ __device__ __forceinline__ u32 instance_of(const u64* __restrict__ base, u32 n, 
     return lo;
 }
 
+// Per-row tables of the instances' bit matrices: row v of instance i (values
+// base[i] .. min(base[i + 1], rows) - 1, words w_i = ceil(n_i / 32) per row) starts at
+// word inst_word[i] + (v - base[i]) * w_i.  `base` holds n_inst + 1 entries (a sentinel last).
+__global__ void __launch_bounds__(kThreads) bitmap_tables_kernel(const u64* __restrict__ base, u32 n_inst,
+                                                                 const u64* __restrict__ inst_word, u64 rows,
+                                                                 u64* __restrict__ row_word, u32* __restrict__ row_base,
+                                                                 u32* __restrict__ row_words, u32* __restrict__ row_inst)
+{
+    for (u64 v = (u64)blockIdx.x * kThreads + threadIdx.x; v < rows; v += (u64)gridDim.x * kThreads) {
+        const u32 i = instance_of(base, n_inst, v);
+        const u64 b = base[i], e = min(base[i + 1], rows), w = v < b ? 0 : (e - b + 31) / 32;
+        // a value below the first instance has no words: every tuple on its row is out of range
+        row_word[v] = v < b ? 0 : inst_word[i] + (v - b) * w;
+        row_base[v] = (u32)b;
+        row_words[v] = (u32)w;
+        row_inst[v] = i;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
                                                           SelectArgs a, const u64* __restrict__ cand,
                                                           const u32* __restrict__ loser,
