@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 ENGINE_SRCS = [os.path.join(HERE, "csrc", "ra_engine.cu")]   # includes csrc/ra_noalloc.cu
 ENGINE_DEPS = ENGINE_SRCS + [os.path.join(HERE, "csrc", f) for f in (
-    "ra_device.cuh", "ra_kernels.cuh", "ra_iter.cuh", "ra_noalloc.cu")] + [
+    "ra_device.cuh", "ra_kernels.cuh", "ra_iter.cuh", "ra_dense.cuh", "ra_noalloc.cu")] + [
     os.path.join(ROOT, "include", "ra_engine.h")]
 ENGINE_LIB = os.path.join(HERE, "libra_b200.so")
 
