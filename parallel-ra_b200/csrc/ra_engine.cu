@@ -2832,10 +2832,14 @@ int ra_relation_instance_summary(ra_program* p, int rel, uint64_t* counts, uint6
         dev_alloc(p, &acc, 2 * m);
         CK(cudaMemsetAsync(acc, 0, 2 * m * 8, p->stream));
         if (r.full_n) {
-            instance_summary_kernel<<<grid_for((r.full_n + kSummaryRowsPerLane - 1) / kSummaryRowsPerLane), kThreads, 0,
-                                      p->stream>>>(
-                r.keys, r.full_n, (int)r.arity, p->bits, p->n_inst ? p->dinst_base : nullptr, p->n_inst, acc,
-                acc + m);
+            const int g = grid_for((r.full_n + kSummaryRowsPerLane - 1) / kSummaryRowsPerLane);
+            const u64* bs = p->n_inst ? p->dinst_base : nullptr;
+            if (r.arity == 2)
+                instance_summary_kernel<2><<<g, kThreads, 0, p->stream>>>(r.keys, r.full_n, 2, p->bits, bs, p->n_inst,
+                                                                           acc, acc + m);
+            else
+                instance_summary_kernel<0><<<g, kThreads, 0, p->stream>>>(r.keys, r.full_n, (int)r.arity, p->bits, bs,
+                                                                           p->n_inst, acc, acc + m);
             LAUNCHED();
         }
         CK(cudaMemcpyAsync(counts, acc, m * 8, cudaMemcpyDeviceToHost, p->stream));

@@ -1123,15 +1123,20 @@ __device__ __forceinline__ u64 tuple_digest(const u64* cols, int arity)
 // instance) of packed rows.  Each warp walks a contiguous segment of rows
 // (coalesced), every lane keeps a running (count, digest) for the instance of
 // its last rows and flushes it when the instance changes; relation logs hold
-// each instance's rows in long runs, so flushes are rare.  Up to
-// kSummarySmemInst instances accumulate in shared memory first.
+// each instance's rows in long runs, so flushes are rare, and a row inside the
+// current instance's value range skips the search over the bases.  Up to
+// kSummarySmemInst instances accumulate in shared memory first.  ARITY > 0
+// fixes the arity at compile time (columns in registers); 0 reads `arity`.
 constexpr u32 kSummarySmemInst = 1024;
 constexpr int kSummaryRowsPerLane = 16;
 
+template <int ARITY>
 __global__ void __launch_bounds__(kThreads) instance_summary_kernel(
-    const u64* __restrict__ keys, u64 n, int arity, int bits, const u64* __restrict__ base, u32 n_inst,
+    const u64* __restrict__ keys, u64 n, int arity_rt, int bits, const u64* __restrict__ base, u32 n_inst,
     u64* __restrict__ counts, u64* __restrict__ digests)
 {
+    const int arity = ARITY > 0 ? ARITY : arity_rt;
+    constexpr int kCols = ARITY > 0 ? ARITY : kMaxArity;
     __shared__ u64 s_cnt[kSummarySmemInst];
     __shared__ u64 s_dig[kSummarySmemInst];
     const u32 m = base ? n_inst : 1;
@@ -1140,6 +1145,7 @@ __global__ void __launch_bounds__(kThreads) instance_summary_kernel(
         for (u32 i = threadIdx.x; i < m; i += blockDim.x) s_cnt[i] = s_dig[i] = 0;
     __syncthreads();
     u32 cur = 0xffffffffu;
+    u64 cur_lo = 1, cur_hi = 0;   // value range of instance `cur` (empty: no instance yet)
     u64 c = 0, dsum = 0;
     auto flush = [&]() {
         if (!c) return;
@@ -1161,15 +1167,22 @@ __global__ void __launch_bounds__(kThreads) instance_summary_kernel(
             const u64 i = w * seg + (u64)j * 32 + lane;
             if (i >= n) break;
             const u64 k = keys[i];
-            u64 cols[kMaxArity];
-            for (int q = 0; q < arity; q++) cols[q] = column_of(k, arity, q, bits);
-            const u32 inst = base ? instance_of(base, n_inst, cols[0]) : 0;
-            if (inst != cur) {
-                flush();
-                cur = inst;
+            u64 cols[kCols];
+#pragma unroll
+            for (int q = 0; q < kCols; q++)
+                if (q < arity) cols[q] = column_of(k, arity, q, bits);
+            if (!(cols[0] >= cur_lo && cols[0] < cur_hi)) {
+                const u32 inst = base ? instance_of(base, n_inst, cols[0]) : 0;
+                if (inst != cur) {
+                    flush();
+                    cur = inst;
+                }
+                cur_lo = base ? __ldg(&base[inst]) : 0;
+                cur_hi = base ? __ldg(&base[inst + 1]) : ~0ull;
             }
-            const u64 b = base ? __ldg(&base[inst]) : 0;
-            for (int q = 0; q < arity; q++) cols[q] -= b;
+#pragma unroll
+            for (int q = 0; q < kCols; q++)
+                if (q < arity) cols[q] -= cur_lo;
             c++;
             dsum += tuple_digest(cols, arity);
         }
