@@ -217,7 +217,9 @@ int ra_scc_depend(ra_program* p, int src_scc, int dst_scc);
 int ra_program_execute(ra_program* p);
 /* One step of LIE::execute's task loop (src/lie/lie.cpp:254-441): run the first
  * runnable SCC (LIE::one_runnable_tasks, lie.cpp:27-60) to its fixed point and
- * store its id in *scc_id, or store -1 when every SCC has run. */
+ * store its id in *scc_id, or store -1 when every SCC has run (that call ends the
+ * run).  Between steps, relation counts are those LIE::execute prints after an
+ * SCC: before that SCC's final delta -> full merge (lie.cpp:432). */
 int ra_program_run_next_scc(ra_program* p, int* scc_id);
 /* Return every relation to its loaded state so the program can run again. */
 int ra_program_reset(ra_program* p);

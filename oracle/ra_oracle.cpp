@@ -22,7 +22,7 @@
 
 namespace {
 
-constexpr int kMaxCols = 8;                 /* arity + 1 <= 8 */
+constexpr int kMaxCols = 64;                /* arity + 1 <= 64 */
 constexpr uint64_t kJoinThreshold = 20000000;   /* src/RAM/RA_tasks.cpp:312 */
 
 using tuple = std::array<uint64_t, kMaxCols>;   /* unused trailing columns are 0 */

@@ -14,6 +14,8 @@
  *   - then RAM::insert_delta_in_full (lie.cpp:432).
  *
  * usage: ref_driver <tc|sg> <edge_file> <empty_file> <out_dir> [batch_size]
+ *        ref_driver file <program.txt> <empty_file> <out_dir> <data_dir>
+ *                   (a program description, its batch size from the file)
  * writes: <out_dir>/history.txt   "scc <id> <iters>" then "<sum_delta> <sum_full>" per batch
  *         <out_dir>/sizes.txt     "<name> <arity> <full_count>" per relation
  *         <out_dir>/<name>.bin    full relation rows (arity+1 u64, trie order = sorted)
@@ -44,7 +46,7 @@ int main(int argc, char** argv)
         return 2;
     }
     std::string prog = argv[1], edge = argv[2], empty = argv[3], out = argv[4];
-    int batch = argc > 5 ? atoi(argv[5]) : 1;
+    int batch = (argc > 5 && prog != "file") ? atoi(argv[5]) : 1;
 
     mpi_comm mcomm;
     mcomm.create(argc, argv);
@@ -53,6 +55,10 @@ int main(int argc, char** argv)
     ra_program_def p;
     if (prog == "tc") build_tc(p, edge, empty);
     else if (prog == "sg") build_sg(p, edge, empty);
+    else if (prog == "file" && argc > 5) {
+        build_from_description(p, edge, argv[5], empty);
+        batch = pd_batch_size(edge);
+    }
     else { fprintf(stderr, "unknown program %s\n", prog.c_str()); return 2; }
 
     for (relation* r : p.relations) {

@@ -59,6 +59,9 @@ REFERENCE = os.environ.get("RA_REFERENCE", "/root/reference")
 BIN_DIR = os.path.join(CXX_DIR, "bin")
 
 
+GENERATED_PROGRAMS = ["worstcase-110-terms-4-m"]
+
+
 def build_reference_programs(force=False):
     """Compile the reference's own program sources, unchanged, against cxx/src.
 
@@ -68,6 +71,8 @@ def build_reference_programs(force=False):
     reference tree exists; the binaries in cxx/bin/ are used elsewhere.
     """
     progs = {"TC": os.path.join(REFERENCE, "tests", "transitive_closure.cpp")}
+    for name in GENERATED_PROGRAMS:   # the reference's generated analyses (wide tuples)
+        progs[name] = os.path.join(REFERENCE, "tests", name + ".cpp")
     os.makedirs(os.path.join(CXX_DIR, "tests"), exist_ok=True)
     os.makedirs(BIN_DIR, exist_ok=True)
     for name, src in progs.items():

@@ -17,6 +17,7 @@
 //     device counters.
 #include "../../include/ra_engine.h"
 #include "ra_dense.cuh"
+#include "ra_wide.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -123,6 +124,16 @@ struct Relation {
     u64 bm_rows = 0;              // capacity of bm_dirty (rows)
     // newt staging for the running iteration
     u64 newt_n = 0;
+    // wide programs: versions as rows of arity + 1 u64 in trie order (counts above)
+    u64* wfull = nullptr;
+    u64* wdelta = nullptr;
+    u64* wnewt = nullptr;
+    u64* wspare = nullptr;   // merge target, swapped with full / delta
+    u64* wcand = nullptr;    // the running iteration's candidates into this relation
+    u32* wflag = nullptr;    // their winner flags
+    u64* wpos = nullptr;     // and the winners' positions
+    u64 wfull_cap = 0, wdelta_cap = 0, wnewt_cap = 0, wspare_cap = 0, wcand_cap = 0, wflag_cap = 0, wpos_cap = 0;
+    int wcand_w = 0;         // columns per candidate row of wcand
 };
 
 }  // namespace
@@ -143,6 +154,9 @@ struct ra_program {
     int bits = 0;                 // packed bits per column for this run
     u64 max_value = 0;            // largest data value loaded (sets `bits`)
     bool packed = false;          // loaded relations packed with `bits` (cleared by a new load)
+    bool wide = false;            // this run keeps tuples as rows of u64 columns (ra_wide.cu)
+    u64* wbuf[12] = {};           // scratch of the wide path
+    u64 wbuf_cap[12] = {};
     bool executed = false;
     bool running = false;         // between the first and the last SCC of a run
     double fixpoint_ms_acc = 0;
@@ -2054,9 +2068,14 @@ bool run_scc_dense(ra_program* p, Scc& s)
 // RAM::insert_delta_in_full of the previous SCC (lie.cpp:436): done when the next SCC
 // starts or the run ends, so that counts read between SCCs are the ones the
 // reference prints there (its size print precedes the merge).
+#include "ra_wide.cu"
+
 void merge_pending(ra_program* p)
 {
-    for (int ri : p->pending_merge) delta_to_full(p->rels[ri]);
+    for (int ri : p->pending_merge) {
+        if (p->wide) wide_delta_to_full(p, p->rels[ri]);
+        else delta_to_full(p->rels[ri]);
+    }
     p->pending_merge.clear();
 }
 
@@ -2068,6 +2087,10 @@ void run_scc(ra_program* p, Scc& s)
             fail(p, RA_E_UNSUPPORTED, "SCC %d: rule output %s is not one of the SCC's relations", s.id,
                  p->rels[ru.out].name.c_str());
     p->loop_counter = 0;
+    if (p->wide) {
+        run_scc_wide(p, s);
+        return;
+    }
     if (!p->rs_dir.empty()) {
         // restart (lie.cpp:300-330): deltas from the dump instead of full -> delta
         for (int ri : s.rels) load_restart_delta(p, p->rels[ri]);
@@ -2124,11 +2147,9 @@ void choose_bits(ra_program* p)
     u64 mx = read_scalar(p, p->dscalar + 1);
     int bits = 1;
     while (bits < 64 && (mx >> bits)) bits++;
-    for (Relation& r : p->rels)
-        if ((int)r.arity * bits > 63)
-            fail(p, RA_E_UNSUPPORTED,
-                 "relation %s: %u columns of %d bits do not pack into one 63-bit key (largest value %llu)",
-                 r.name.c_str(), r.arity, bits, (unsigned long long)mx);
+    // tuples that do not pack into one 63-bit key (or joins the CSR index cannot
+    // hold) run on the wide path
+    p->wide = program_needs_wide(p, bits);
     p->bits = bits;
     p->max_value = mx;
 }
@@ -2146,6 +2167,7 @@ void free_relation_state(ra_program* p, Relation& r)
     dev_free(p, &r.bm_fresh);
     dev_free(p, &r.bm_dirty);
     r.bm_rows = r.bm_words = 0;
+    wide_free_relation(p, r);
     r.cap = r.seen_cap = r.seen_n = r.v_cap = r.csr_full_cap = r.csr_delta_cap = 0;
     r.v_version = r.csr_full_version = r.csr_delta_version = ~0ull;
     r.full_n = r.delta_n = r.newt_n = 0;
@@ -2222,6 +2244,10 @@ void release_buffers(ra_program* p)
     dev_free(p, &p->bmt_inst);
     p->bmt_rows = 0;
     p->bmt_bases.clear();
+    for (int i = 0; i < 12; i++) {
+        dev_free(p, &p->wbuf[i]);
+        p->wbuf_cap[i] = 0;
+    }
     for (Scc& sc : p->sccs) drop_graph(sc);
     CK(cudaStreamSynchronize(p->stream));
 }
@@ -2238,10 +2264,17 @@ void begin_run(ra_program* p)
     p->dedup_events.clear();
     if (!p->packed) {
         choose_bits(p);
-        for (Relation& r : p->rels) pack_relation(p, r);
+        if (!p->wide)
+            for (Relation& r : p->rels) pack_relation(p, r);
         p->packed = true;
-    } else {
+    } else if (!p->wide) {
         for (Relation& r : p->rels) restore_loaded(p, r);
+    }
+    if (p->wide) {
+        if (p->n_inst) fail(p, RA_E_UNSUPPORTED, "batched instances of a wide-tuple program");
+        if (p->cp_every || !p->rs_dir.empty())
+            fail(p, RA_E_UNSUPPORTED, "checkpoint dumps or restart of a wide-tuple program");
+        for (Relation& r : p->rels) wide_load(p, r);
     }
     p->running = true;
     p->fixpoint_ms_acc = 0;
@@ -2313,7 +2346,8 @@ int step(ra_program* p)
     float ms = 0;
     cudaEventElapsedTime(&ms, p->ev0, p->ev1);
     p->fixpoint_ms_acc += ms;
-    if (next_runnable(p) < 0) finish_run(p);
+    // the run ends at the next step, so that counts read after the last SCC are, as
+    // the reference prints them there, from before its final delta -> full merge
     return p->sccs[next].id;
 }
 
@@ -2491,8 +2525,8 @@ int ra_relation_create(ra_program* p, uint32_t jcc, uint32_t arity, uint32_t tag
                        int* rel_out)
 {
     return guard(p, [&] {
-        if (!rel_out || arity == 0 || arity > (uint32_t)kMaxArity || jcc == 0 || jcc > arity)
-            fail(p, RA_E_BADARG, "relation: need 1 <= jcc <= arity <= %d", kMaxArity);
+        if (!rel_out || arity == 0 || arity >= (uint32_t)kWideMaxCols || jcc > arity)
+            fail(p, RA_E_BADARG, "relation: need 0 <= jcc <= arity <= %d", kWideMaxCols - 1);
         if (version != RA_DELTA && version != RA_FULL) fail(p, RA_E_BADARG, "relation: version must be DELTA or FULL");
         if (tag >= (1u << 18)) fail(p, RA_E_BADARG, "relation: intern tag must be below 2^18");
         Relation r;
@@ -2605,7 +2639,7 @@ int ra_scc_add_join(ra_program* p, int scc, int out, int in0, int ver0, int in1,
         rel_at(p, in1);
         if ((ver0 != RA_DELTA && ver0 != RA_FULL) || (ver1 != RA_DELTA && ver1 != RA_FULL))
             fail(p, RA_E_BADARG, "join versions must be DELTA or FULL");
-        if (nproj <= 0 || nproj > kMaxArity || !proj) fail(p, RA_E_BADARG, "join projection size");
+        if (nproj <= 0 || nproj >= kWideMaxCols || !proj) fail(p, RA_E_BADARG, "join projection size");
         Rule r{kJoin, out, in0, ver0, in1, ver1, std::vector<int>(proj, proj + nproj), 0};
         s.rules.push_back(r);
     });
@@ -2619,7 +2653,7 @@ int ra_scc_add_copy(ra_program* p, int scc, int kind, int out, int in, int ver, 
         rel_at(p, in);
         if (kind != RA_COPY && kind != RA_ACOPY && kind != RA_COPY_FILTER) fail(p, RA_E_BADARG, "copy kind");
         if (ver != RA_DELTA && ver != RA_FULL) fail(p, RA_E_BADARG, "copy version must be DELTA or FULL");
-        if (nproj <= 0 || nproj > kMaxArity + 1 || !proj) fail(p, RA_E_BADARG, "copy reorder size");
+        if (nproj <= 0 || nproj > kWideMaxCols || !proj) fail(p, RA_E_BADARG, "copy reorder size");
         if (kind == RA_COPY_FILTER && (pred < RA_PRED_TRUE || pred > RA_PRED_GE)) fail(p, RA_E_BADARG, "predicate");
         Rule r{kind, out, in, ver, -1, -1, std::vector<int>(proj, proj + nproj), kind == RA_COPY_FILTER ? pred : 0};
         s.rules.push_back(r);
@@ -2831,7 +2865,14 @@ int ra_relation_instance_summary(ra_program* p, int rel, uint64_t* counts, uint6
         u64* acc;
         dev_alloc(p, &acc, 2 * m);
         CK(cudaMemsetAsync(acc, 0, 2 * m * 8, p->stream));
-        if (r.full_n) {
+        if (p->wide) {   // one instance (a wide program declares none)
+            CK(cudaMemcpyAsync(acc, &r.full_n, 8, cudaMemcpyHostToDevice, p->stream));
+            if (r.full_n) {
+                wide_summary_kernel<<<wide_grid(r.full_n), kThreads, 0, p->stream>>>(r.wfull, (int)r.arity + 1,
+                                                                                      r.full_n, acc);
+                LAUNCHED();
+            }
+        } else if (r.full_n) {
             const int g = grid_for((r.full_n + kSummaryRowsPerLane - 1) / kSummaryRowsPerLane);
             const u64* bs = p->n_inst ? p->dinst_base : nullptr;
             if (r.arity == 2)
@@ -2871,6 +2912,14 @@ int ra_relation_dump_full(ra_program* p, int rel, uint64_t* host_rows, uint64_t 
     return guard(p, [&] {
         Relation& r = rel_at(p, rel);
         if (!p->executed) fail(p, RA_E_STATE, "dump before execute");
+        if (p->wide) {   // rows already in trie order
+            const u64 m = std::min<u64>(r.full_n, cap_rows);
+            if (rows_out) *rows_out = m;
+            if (m && host_rows)
+                CK(cudaMemcpyAsync(host_rows, r.wfull, m * (r.arity + 1) * 8, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+            return;
+        }
         const u64 *k, *v;
         u64 n;
         version_rows(p, r, RA_FULL, &k, &v, &n);

@@ -1,0 +1,447 @@
+// Host side of the wide-tuple path (kernels in ra_wide.cuh).  Included into
+// ra_engine.cu's translation unit: it uses ra_program, Relation and the
+// engine's allocation, scan and error helpers.
+//
+// A program runs wide when some relation's tuples do not pack into one 63-bit
+// key, a relation has more than kMaxArity columns or joins on zero columns, or
+// a join key exceeds the CSR index's 30 bits.  Every relation version is then an
+// array of arity + 1 u64 rows in trie order, and one iteration of an SCC is
+// RAM::local_compute + local_insert_in_newt + local_insert_in_full
+// (src/RAM/RA_tasks.cpp:305-555, 824-905; balanced_hash_relation.cpp:1120-1231):
+//   1. each rule's candidates, in the reference's emission order (outer rows in
+//      trie order, each one's inner matches in trie order; copies in input order),
+//      written into its output relation's candidate buffer after the earlier rules';
+//   2. per output relation: an index sort of the candidates by (data columns,
+//      position); the first of each group wins unless full or delta holds it;
+//   3. ids (tag << 46) | counter assigned to the winners rule by rule in the SCC's
+//      rule order, the counters shared by the relations of one tag, as the
+//      single-rank reference interns them (bucket 0);
+//   4. newt sorted into trie order; full = full + delta (a rank merge), delta = newt.
+// Intern ids therefore equal the reference's, and with them every data column
+// that a rule copies out of an id (acopy).
+//
+// (Included inside the engine's anonymous namespace.)
+
+// Scratch slots of the wide path (grow-only, contents not kept across calls).
+enum WideSlot { kWsIdxA, kWsIdxB, kWsRows, kWsLo, kWsCnt, kWsOff, kWsPos, kWsFlag, kWsSmall, kWsCount };
+static_assert(kWsCount <= 12, "wide scratch slots");
+
+u64* wide_scratch(ra_program* p, int slot, u64 n)
+{
+    if (n > p->wbuf_cap[slot]) {
+        dev_free(p, &p->wbuf[slot]);
+        p->wbuf_cap[slot] = 0;
+        const u64 nc = std::max<u64>(n + n / 2, 4096);
+        dev_alloc(p, &p->wbuf[slot], nc);
+        p->wbuf_cap[slot] = nc;
+    }
+    return p->wbuf[slot];
+}
+
+u32* wide_scratch32(ra_program* p, int slot, u64 n) { return (u32*)wide_scratch(p, slot, (n + 1) / 2); }
+
+// Room for `rows` rows of W columns in *buf, keeping the first keep_rows rows.
+void wide_reserve(ra_program* p, u64** buf, u64* cap, u64 rows, int W, u64 keep_rows)
+{
+    if (rows <= *cap && *buf) return;
+    const u64 nc = std::max<u64>(rows + rows / 2, 256);
+    *cap = std::min<u64>(*cap, keep_rows);   // a failed allocation leaves no stale capacity
+    u64* nb;
+    dev_alloc(p, &nb, nc * (u64)W);
+    if (keep_rows && *buf) CK(cudaMemcpyAsync(nb, *buf, keep_rows * (u64)W * 8, cudaMemcpyDeviceToDevice, p->stream));
+    dev_free(p, buf);
+    *buf = nb;
+    *cap = nc;
+}
+
+// Room for n u32 flags in *buf (contents not kept).
+void wide_reserve32(ra_program* p, u32** buf, u64* cap, u64 n)
+{
+    if (n <= *cap && *buf) return;
+    dev_free(p, buf);
+    *cap = 0;
+    const u64 nc = std::max<u64>(n + n / 2, 1024);
+    dev_alloc(p, buf, nc);
+    *cap = nc;
+}
+
+int wide_grid(u64 n) { return grid_for(std::max<u64>(n, 1)); }
+
+// Indices 0..n-1 of `rows` sorted by (first ncmp columns, index); the result is
+// one of the two index scratch slots.
+const u64* wide_sort(ra_program* p, const u64* rows, int W, int ncmp, u64 n)
+{
+    u64* a = wide_scratch(p, kWsIdxA, n);
+    u64* b = wide_scratch(p, kWsIdxB, n);
+    const u64 tiles = (n + kWideSortTile - 1) / kWideSortTile;
+    wide_tile_sort_kernel<<<(unsigned)tiles, kThreads, 0, p->stream>>>(rows, W, ncmp, n, a);
+    LAUNCHED();
+    for (u64 L = kWideSortTile; L < n; L *= 2) {
+        wide_merge_pass_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(rows, W, ncmp, n, L, a, b);
+        LAUNCHED();
+        std::swap(a, b);
+    }
+    return a;
+}
+
+// Rows of `src` (n rows of W columns) sorted into trie order and made distinct,
+// into *dst (capacity *cap); returns the row count.
+u64 wide_sort_unique(ra_program* p, const u64* src, int W, u64 n, u64** dst, u64* cap)
+{
+    if (!n) return 0;
+    const u64* idx = wide_sort(p, src, W, W, n);
+    wide_reserve(p, dst, cap, n, W, 0);
+    wide_gather_kernel<<<wide_grid(n * W), kThreads, 0, p->stream>>>(src, W, idx, n, *dst);
+    LAUNCHED();
+    u32* keep = wide_scratch32(p, kWsFlag, n);
+    CK(cudaMemsetAsync(p->derr, 0, 4, p->stream));
+    wide_dup_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(*dst, W, n, keep, p->derr);
+    LAUNCHED();
+    if (!(read_scalar(p, (const u64*)p->derr) & 0xffffffffull)) return n;
+    u64* pos = wide_scratch(p, kWsPos, n);
+    const u64 m = scan_exclusive<u32>(p, keep, n, pos);
+    u64* tmp = wide_scratch(p, kWsRows, n * W);
+    wide_compact_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(*dst, W, n, keep, pos, tmp);
+    LAUNCHED();
+    CK(cudaMemcpyAsync(*dst, tmp, m * (u64)W * 8, cudaMemcpyDeviceToDevice, p->stream));
+    return m;
+}
+
+// *a = *a + b (both sorted, in trie order); the merged rows go to the spare
+// buffer, which then becomes *a.
+void wide_merge_into(ra_program* p, Relation& r, u64** a, u64* acap, u64* an, const u64* b, u64 bn)
+{
+    const int W = (int)r.arity + 1;
+    if (!bn) return;
+    if (!*an) {
+        wide_reserve(p, a, acap, bn, W, 0);
+        CK(cudaMemcpyAsync(*a, b, bn * (u64)W * 8, cudaMemcpyDeviceToDevice, p->stream));
+        *an = bn;
+        return;
+    }
+    const u64 n = *an + bn;
+    wide_reserve(p, &r.wspare, &r.wspare_cap, n, W, 0);
+    wide_merge_rows_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(*a, *an, b, bn, W, r.wspare);
+    LAUNCHED();
+    std::swap(*a, r.wspare);
+    std::swap(*acap, r.wspare_cap);
+    *an = n;
+}
+
+// relation::insert_delta_in_full (balanced_hash_relation.cpp:1120-1148)
+void wide_delta_to_full(ra_program* p, Relation& r)
+{
+    if (!r.delta_n) return;
+    wide_merge_into(p, r, &r.wfull, &r.wfull_cap, &r.full_n, r.wdelta, r.delta_n);
+    r.delta_n = 0;
+}
+
+// relation::insert_full_in_delta (balanced_hash_relation.cpp:1152-1179)
+void wide_full_to_delta(ra_program* p, Relation& r)
+{
+    if (!r.full_n) return;
+    wide_merge_into(p, r, &r.wdelta, &r.wdelta_cap, &r.delta_n, r.wfull, r.full_n);
+    r.full_n = 0;
+}
+
+// Loaded rows (arity + 1 columns) into the relation's loaded version, in trie
+// order and distinct on all columns, as populate_full inserts them
+// (balanced_hash_relation.cpp:609-793).
+void wide_load(ra_program* p, Relation& r)
+{
+    r.full_n = r.delta_n = r.newt_n = 0;
+    if (!r.raw_n) return;
+    const int W = (int)r.arity + 1;
+    if (r.version == RA_DELTA) r.delta_n = wide_sort_unique(p, r.raw, W, r.raw_n, &r.wdelta, &r.wdelta_cap);
+    else r.full_n = wide_sort_unique(p, r.raw, W, r.raw_n, &r.wfull, &r.wfull_cap);
+}
+
+// The rows of one version of a relation (sorted).
+const u64* wide_version(Relation& r, int ver, u64* n)
+{
+    *n = ver == RA_DELTA ? r.delta_n : r.full_n;
+    return ver == RA_DELTA ? r.wdelta : r.wfull;
+}
+
+// Candidate width of a relation written by an SCC's rules: data columns, or all
+// columns for acopy targets (which carry their last column from the input).
+int wide_cand_width(ra_program* p, const Scc& s, int out)
+{
+    int acopy = -1;
+    for (const Rule& ru : s.rules) {
+        if (ru.out != out) continue;
+        const int a = ru.kind == RA_ACOPY ? 1 : 0;
+        if (acopy >= 0 && acopy != a)
+            fail(p, RA_E_UNSUPPORTED, "SCC %d: relation %s is written by acopy and by other rules", s.id,
+                 p->rels[out].name.c_str());
+        acopy = a;
+    }
+    return (int)p->rels[out].arity + (acopy == 1 ? 1 : 0);
+}
+
+// Projection of a rule onto its output's candidate columns, checked against the inputs.
+WideProj wide_proj(ra_program* p, const Scc& s, const Rule& ru, int cw)
+{
+    WideProj pj{};
+    const Relation& o = p->rels[ru.out];
+    const Relation& a = p->rels[ru.in0];
+    pj.n = (int)ru.proj.size();
+    if (pj.n != cw || pj.n > kWideMaxCols)
+        fail(p, RA_E_BADARG, "SCC %d: a rule into %s projects %d columns, the relation takes %d", s.id, o.name.c_str(),
+             pj.n, cw);
+    int span;
+    if (ru.kind == kJoin) {
+        const Relation& b = p->rels[ru.in1];
+        if (a.jcc != b.jcc || a.jcc > a.arity || a.jcc > b.arity)
+            fail(p, RA_E_BADARG, "SCC %d: join of %s and %s on different join columns", s.id, a.name.c_str(),
+                 b.name.c_str());
+        pj.left = ru.ver0 == RA_DELTA ? 1 : 0;
+        pj.W0 = (int)a.arity + 1;
+        pj.W1 = (int)b.arity + 1;
+        pj.jcc = (int)a.jcc;
+        span = pj.W0 + pj.W1 - pj.jcc;
+    } else {
+        span = (int)a.arity + 1;
+    }
+    for (int j = 0; j < pj.n; j++) {
+        if (ru.proj[j] < 0 || ru.proj[j] >= span)
+            fail(p, RA_E_BADARG, "SCC %d: projection column %d outside the rule's %d input columns", s.id, ru.proj[j],
+                 span);
+        pj.src[j] = ru.proj[j];
+    }
+    return pj;
+}
+
+struct WideOut {
+    int rel;
+    int cw;
+    u64 n = 0;                      // candidates so far
+    std::vector<int> rules;         // rule index of each segment
+    std::vector<u64> seg_start;     // first candidate of each segment
+    u64 winners = 0;
+    std::vector<u64> seg_wins;      // winners before each segment, then the total
+};
+
+// One iteration: RAM::local_compute + local_insert_in_newt + local_insert_in_full.
+void wide_iteration(ra_program* p, Scc& s)
+{
+    std::vector<WideOut> outs;
+    outs.reserve(s.rules.size());
+    auto out_of = [&](int rel) -> WideOut& {
+        for (WideOut& o : outs)
+            if (o.rel == rel) return o;
+        WideOut o;
+        o.rel = rel;
+        o.cw = wide_cand_width(p, s, rel);
+        Relation& R = p->rels[rel];
+        if (R.wcand_w != o.cw) {   // the buffer's capacity counts rows of its last width
+            dev_free(p, &R.wcand);
+            R.wcand_cap = 0;
+            R.wcand_w = o.cw;
+        }
+        outs.push_back(o);
+        return outs.back();
+    };
+    // 1. candidates, rule by rule
+    for (size_t q = 0; q < s.rules.size(); q++) {
+        const Rule& ru = s.rules[q];
+        WideOut& wo = out_of(ru.out);
+        Relation& R = p->rels[ru.out];
+        const WideProj pj = wide_proj(p, s, ru, wo.cw);
+        if ((int)wo.rules.size() >= kWideMaxSegs)
+            fail(p, RA_E_UNSUPPORTED, "SCC %d: more than %d rules write relation %s", s.id, kWideMaxSegs,
+                 R.name.c_str());
+        wo.rules.push_back((int)q);
+        wo.seg_start.push_back(wo.n);
+        if (ru.kind == kJoin) {
+            Relation& a = p->rels[ru.in0];
+            Relation& b = p->rels[ru.in1];
+            u64 no, ni;
+            const u64 *outer, *inner;
+            if (ru.ver0 == RA_DELTA) {
+                outer = wide_version(a, RA_DELTA, &no);
+                inner = wide_version(b, ru.ver1, &ni);
+            } else {
+                outer = wide_version(b, ru.ver1, &no);
+                inner = wide_version(a, RA_FULL, &ni);
+            }
+            if (!no || !ni) continue;
+            u64* lo = wide_scratch(p, kWsLo, no);
+            u64* cnt = wide_scratch(p, kWsCnt, no);
+            u64* off = wide_scratch(p, kWsOff, no);
+            const int Wo = pj.left ? pj.W0 : pj.W1, Wi = pj.left ? pj.W1 : pj.W0;
+            wide_join_count_kernel<<<wide_grid(no), kThreads, 0, p->stream>>>(outer, Wo, no, inner, Wi, ni, pj.jcc, lo,
+                                                                              cnt);
+            LAUNCHED();
+            const u64 total = scan_exclusive<u64>(p, cnt, no, off);
+            if (!total) continue;
+            wide_reserve(p, &R.wcand, &R.wcand_cap, wo.n + total, wo.cw, wo.n);
+            wide_join_expand_kernel<<<wide_grid(total), kThreads, 0, p->stream>>>(
+                outer, inner, no, lo, off, total, pj, R.wcand + wo.n * (u64)wo.cw);
+            LAUNCHED();
+            wo.n += total;
+            p->stats.join_candidates += total;
+        } else {
+            Relation& a = p->rels[ru.in0];
+            u64 n;
+            const u64* in = wide_version(a, ru.ver0, &n);
+            if (!n) continue;
+            const int Wi = (int)a.arity + 1;
+            u64 m = n;
+            u32* keep = nullptr;
+            u64* pos = nullptr;
+            if (ru.kind == RA_COPY_FILTER) {
+                keep = wide_scratch32(p, kWsFlag, n);
+                pos = wide_scratch(p, kWsPos, n);
+                wide_filter_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(in, Wi, n, ru.pred, keep);
+                LAUNCHED();
+                m = scan_exclusive<u32>(p, keep, n, pos);
+                if (!m) continue;
+            }
+            wide_reserve(p, &R.wcand, &R.wcand_cap, wo.n + m, wo.cw, wo.n);
+            wide_copy_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(in, Wi, n, pj, keep, pos,
+                                                                       R.wcand + wo.n * (u64)wo.cw);
+            LAUNCHED();
+            wo.n += m;
+        }
+    }
+    // 2. winners per output relation
+    for (WideOut& wo : outs) {
+        Relation& R = p->rels[wo.rel];
+        wo.seg_wins.assign(wo.rules.size() + 1, 0);
+        if (!wo.n) continue;
+        const int W = (int)R.arity + 1;
+        const u64* idx = wide_sort(p, R.wcand, wo.cw, wo.cw, wo.n);
+        wide_reserve32(p, &R.wflag, &R.wflag_cap, wo.n);
+        wide_reserve(p, &R.wpos, &R.wpos_cap, wo.n, 1, 0);
+        wide_winner_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, idx, wo.n, R.wfull, R.full_n,
+                                                                        R.wdelta, R.delta_n, W, R.wflag);
+        LAUNCHED();
+        wo.winners = scan_exclusive<u32>(p, R.wflag, wo.n, R.wpos);
+        WideSegs sg{};
+        sg.n = (int)wo.rules.size();
+        for (int k = 0; k < sg.n; k++) sg.start[k] = wo.seg_start[k];
+        sg.start[sg.n] = wo.n;
+        u64* small = wide_scratch(p, kWsSmall, kWideMaxSegs + 1);
+        wide_pick_kernel<<<1, kWideMaxSegs + 1, 0, p->stream>>>(R.wpos, wo.n, wo.winners, sg, small);
+        LAUNCHED();
+        CK(cudaMemcpyAsync(wo.seg_wins.data(), small, (sg.n + 1) * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        // the newt rows need the ids of every relation's earlier rules: after all relations
+        R.newt_n = wo.winners;
+        if (wo.winners) wide_reserve(p, &R.wnewt, &R.wnewt_cap, wo.winners, W, 0);
+    }
+    // 3. ids: rule by rule in the SCC's order, each tag's counter shared by its relations
+    std::vector<u64> id_base(s.rules.size(), 0);
+    for (size_t q = 0; q < s.rules.size(); q++) {
+        const Rule& ru = s.rules[q];
+        if (ru.kind == RA_ACOPY) continue;
+        WideOut& wo = out_of(ru.out);
+        const size_t k = std::find(wo.rules.begin(), wo.rules.end(), (int)q) - wo.rules.begin();
+        const u64 wins = wo.seg_wins[k + 1] - wo.seg_wins[k];
+        u64& ctr = intern_counter(p, p->rels[ru.out].tag);
+        id_base[q] = ((u64)p->rels[ru.out].tag << 46) | ctr;
+        ctr += wins;
+    }
+    // 4. newt rows, sorted into trie order
+    for (WideOut& wo : outs) {
+        Relation& R = p->rels[wo.rel];
+        if (!wo.winners) continue;
+        const int W = (int)R.arity + 1;
+        WideSegs sg{};
+        sg.n = (int)wo.rules.size();
+        for (int k = 0; k < sg.n; k++) {
+            sg.start[k] = wo.seg_start[k];
+            sg.win_base[k] = wo.seg_wins[k];
+            sg.id_base[k] = id_base[wo.rules[k]];
+        }
+        sg.start[sg.n] = wo.n;
+        u64* rows = wide_scratch(p, kWsRows, wo.winners * (u64)W);
+        wide_newt_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, wo.n, R.wflag, R.wpos, sg, W,
+                                                                       rows);
+        LAUNCHED();
+        const u64* idx = wide_sort(p, rows, W, W, wo.winners);
+        wide_gather_kernel<<<wide_grid(wo.winners * W), kThreads, 0, p->stream>>>(rows, W, idx, wo.winners, R.wnewt);
+        LAUNCHED();
+        p->stats.new_tuples += wo.winners;
+    }
+    // local_insert_in_full: full = full + delta, delta = newt
+    for (int ri : s.rels) {
+        Relation& R = p->rels[ri];
+        wide_delta_to_full(p, R);
+        std::swap(R.wdelta, R.wnewt);
+        std::swap(R.wdelta_cap, R.wnewt_cap);
+        R.delta_n = R.newt_n;
+        R.newt_n = 0;
+    }
+    p->stats.iterations++;
+}
+
+// RAM::execute_in_batches driven by LIE::execute (lie.cpp:355-432) for one SCC.
+void run_scc_wide(ra_program* p, Scc& s)
+{
+    for (size_t i = 0; i < s.rels.size(); i++)
+        if (s.init[i]) wide_full_to_delta(p, p->rels[s.rels[i]]);
+    std::vector<uint64_t> hist;
+    for (;;) {
+        uint32_t b = p->batch_size;
+        while (b != 0) {
+            wide_iteration(p, s);
+            b--;
+            if (!s.fixpoint) break;
+        }
+        uint32_t d = 0, f = 0;
+        for (int ri : s.rels) {
+            d += (uint32_t)p->rels[ri].delta_n;
+            f += (uint32_t)p->rels[ri].full_n;
+        }
+        hist.push_back(d);
+        hist.push_back(f);
+        if (!s.fixpoint || d == 0) break;
+    }
+    CK(cudaStreamSynchronize(p->stream));
+    p->pending_merge = s.rels;
+    p->history.push_back((uint64_t)s.id);
+    p->history.push_back(hist.size() / 2);
+    p->history.insert(p->history.end(), hist.begin(), hist.end());
+}
+
+// Does this program need the wide path?  (The packed path's limits: arity and
+// projections of at most kMaxArity columns, joins on at least one column, tuples
+// within 63 packed bits, join keys within the CSR index's 30 bits.)
+bool program_needs_wide(ra_program* p, int bits)
+{
+    for (const Relation& r : p->rels) {
+        if (r.arity > (uint32_t)kMaxArity || r.jcc == 0) return true;
+        if ((int)r.arity * bits > 63) return true;
+    }
+    for (const Scc& s : p->sccs)
+        for (const Rule& ru : s.rules) {
+            if (ru.proj.size() > (size_t)kMaxArity + (ru.kind == RA_ACOPY ? 1 : 0)) return true;
+            const Relation& a = p->rels[ru.in0];
+            if (ru.kind == kJoin) {
+                const Relation& b = p->rels[ru.in1];
+                if ((int)a.jcc * bits > 30) return true;
+                // an intern id projected into a data column
+                const int id0 = (int)a.arity, id1 = (int)(a.arity + 1 + b.arity - a.jcc);
+                for (int x : ru.proj)
+                    if (x == id0 || x == id1) return true;
+            } else if (ru.kind != RA_ACOPY) {
+                for (int x : ru.proj)
+                    if (x == (int)a.arity) return true;
+            }
+        }
+    return false;
+}
+
+void wide_free_relation(ra_program* p, Relation& r)
+{
+    dev_free(p, &r.wfull);
+    dev_free(p, &r.wdelta);
+    dev_free(p, &r.wnewt);
+    dev_free(p, &r.wspare);
+    dev_free(p, &r.wcand);
+    dev_free(p, &r.wflag);
+    dev_free(p, &r.wpos);
+    r.wfull_cap = r.wdelta_cap = r.wnewt_cap = r.wspare_cap = r.wcand_cap = r.wflag_cap = r.wpos_cap = 0;
+}

@@ -1,0 +1,344 @@
+// Wide tuples: programs whose tuples do not pack into one 63-bit key (arity x
+// value bits > 63, e.g. the slog-generated analyses whose columns hold intern
+// ids) or whose join keys exceed the CSR index.  A relation version is an array
+// of rows of arity + 1 u64 (data columns, then the id) in trie order --
+// lexicographic over all columns, the order in which the reference's tries
+// enumerate tuples (src/relation/shmap_relation_exp.cpp:77-112).
+//
+// Operations are index sorts with a row comparator (bitonic tiles in shared
+// memory, then merge passes by binary-searched ranks), prefix binary searches
+// (join ranges on the first jcc columns; membership on the data columns), and
+// rank merges of sorted arrays.  All integer, HBM/L2-bound.
+#pragma once
+
+#include "ra_iter.cuh"
+
+namespace ra {
+
+constexpr int kWideMaxCols = 64;     // arity + 1 columns at most
+constexpr int kWideSortTile = 1024;  // indices sorted per block before the merge passes
+constexpr int kWideMaxSegs = 32;     // rules writing one relation within an SCC
+
+// Lexicographic compare of two rows over their first `ncmp` columns: -1, 0, 1.
+__device__ __forceinline__ int wide_cmp(const u64* __restrict__ a, const u64* __restrict__ b, int ncmp)
+{
+    for (int c = 0; c < ncmp; c++) {
+        const u64 x = a[c], y = b[c];
+        if (x != y) return x < y ? -1 : 1;
+    }
+    return 0;
+}
+
+// Strict total order on row indices: the first `ncmp` columns, then the index.
+__device__ __forceinline__ bool wide_before(const u64* __restrict__ rows, int W, int ncmp, u64 i, u64 j)
+{
+    const int c = wide_cmp(rows + i * W, rows + j * W, ncmp);
+    return c < 0 || (c == 0 && i < j);
+}
+
+// Tile sort: indices [tile * kWideSortTile, ...) of `n` rows, bitonic network in
+// shared memory (missing entries are a sentinel that orders last).
+__global__ void __launch_bounds__(kThreads) wide_tile_sort_kernel(const u64* __restrict__ rows, int W, int ncmp,
+                                                                  u64 n, u64* __restrict__ idx)
+{
+    __shared__ u64 s[kWideSortTile];
+    const u64 base = (u64)blockIdx.x * kWideSortTile;
+    for (int t = threadIdx.x; t < kWideSortTile; t += kThreads) {
+        const u64 g = base + t;
+        s[t] = g < n ? g : ~0ull;
+    }
+    __syncthreads();
+    for (int k = 2; k <= kWideSortTile; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < kWideSortTile; t += kThreads) {
+                const int partner = t ^ j;
+                if (partner <= t) continue;
+                const u64 a = s[t], b = s[partner];
+                bool a_after_b;
+                if (a == ~0ull) a_after_b = b != ~0ull;
+                else if (b == ~0ull) a_after_b = false;
+                else a_after_b = wide_before(rows, W, ncmp, b, a);
+                if (a_after_b == ((t & k) == 0)) {
+                    s[t] = b;
+                    s[partner] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int t = threadIdx.x; t < kWideSortTile; t += kThreads) {
+        const u64 g = base + t;
+        if (g < n) idx[g] = s[t];
+    }
+}
+
+// One merge pass: sorted runs of length L in `in`, pairs merged into `out`.  An
+// element's output position is its offset in its run plus its rank in the
+// partner run (the order is strict, so the ranks of both runs interleave exactly).
+__global__ void __launch_bounds__(kThreads) wide_merge_pass_kernel(const u64* __restrict__ rows, int W, int ncmp,
+                                                                   u64 n, u64 L, const u64* __restrict__ in,
+                                                                   u64* __restrict__ out)
+{
+    for (u64 p = (u64)blockIdx.x * kThreads + threadIdx.x; p < n; p += (u64)gridDim.x * kThreads) {
+        const u64 start = (p / (2 * L)) * 2 * L;
+        const u64 mid = min(start + L, n), end = min(start + 2 * L, n);
+        const u64 v = in[p];
+        const bool left = p < mid;
+        u64 a = left ? mid : start, b = left ? end : mid;
+        const u64 lo = a;
+        while (a < b) {
+            const u64 m = (a + b) >> 1;
+            if (wide_before(rows, W, ncmp, in[m], v)) a = m + 1;
+            else b = m;
+        }
+        out[start + (p - (left ? start : mid)) + (a - lo)] = v;
+    }
+}
+
+// out row k = rows[idx[k]] (W columns), one thread per column value.
+__global__ void __launch_bounds__(kThreads) wide_gather_kernel(const u64* __restrict__ rows, int W,
+                                                               const u64* __restrict__ idx, u64 n,
+                                                               u64* __restrict__ out)
+{
+    const u64 total = n * (u64)W;
+    for (u64 e = (u64)blockIdx.x * kThreads + threadIdx.x; e < total; e += (u64)gridDim.x * kThreads) {
+        const u64 k = e / (u64)W, c = e - k * (u64)W;
+        out[e] = rows[idx[k] * (u64)W + c];
+    }
+}
+
+// First row of each group of equal first-`ncmp`-column rows, in sorted order.
+__global__ void __launch_bounds__(kThreads) wide_head_kernel(const u64* __restrict__ rows, int W, int ncmp,
+                                                             const u64* __restrict__ idx, u64 n,
+                                                             u32* __restrict__ head)
+{
+    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
+        const u64* r = rows + idx[k] * (u64)W;
+        head[k] = (k == 0 || wide_cmp(rows + idx[k - 1] * (u64)W, r, ncmp) != 0) ? 1u : 0u;
+    }
+}
+
+// First row of `sorted` (n rows of Ws columns) whose first `ncmp` columns are not
+// below `key`'s.
+__device__ __forceinline__ u64 wide_lower_bound(const u64* __restrict__ sorted, int Ws, u64 n,
+                                                const u64* __restrict__ key, int ncmp)
+{
+    u64 a = 0, b = n;
+    while (a < b) {
+        const u64 m = (a + b) >> 1;
+        if (wide_cmp(sorted + m * (u64)Ws, key, ncmp) < 0) a = m + 1;
+        else b = m;
+    }
+    return a;
+}
+
+__device__ __forceinline__ u64 wide_upper_bound(const u64* __restrict__ sorted, int Ws, u64 n,
+                                                const u64* __restrict__ key, int ncmp)
+{
+    u64 a = 0, b = n;
+    while (a < b) {
+        const u64 m = (a + b) >> 1;
+        if (wide_cmp(sorted + m * (u64)Ws, key, ncmp) <= 0) a = m + 1;
+        else b = m;
+    }
+    return a;
+}
+
+// Does `sorted` hold a row whose first `ncmp` columns equal `key`'s
+// (relation::find_in_full / find_in_delta, balanced_hash_relation.cpp:1015-1035)?
+__device__ __forceinline__ bool wide_has_prefix(const u64* __restrict__ sorted, int Ws, u64 n,
+                                                const u64* __restrict__ key, int ncmp)
+{
+    if (!n) return false;
+    const u64 i = wide_lower_bound(sorted, Ws, n, key, ncmp);
+    return i < n && wide_cmp(sorted + i * (u64)Ws, key, ncmp) == 0;
+}
+
+// Join ranges: per outer row, the inner rows (trie order) sharing its first jcc
+// columns -- all of them when jcc is 0 (parallel_join::local_join,
+// src/RA/parallel_join.cpp:157-230).
+__global__ void __launch_bounds__(kThreads) wide_join_count_kernel(const u64* __restrict__ outer, int Wo, u64 no,
+                                                                   const u64* __restrict__ inner, int Wi, u64 ni,
+                                                                   int jcc, u64* __restrict__ lo, u64* __restrict__ cnt)
+{
+    for (u64 o = (u64)blockIdx.x * kThreads + threadIdx.x; o < no; o += (u64)gridDim.x * kThreads) {
+        const u64* key = outer + o * (u64)Wo;
+        const u64 a = jcc ? wide_lower_bound(inner, Wi, ni, key, jcc) : 0;
+        const u64 b = jcc ? wide_upper_bound(inner, Wi, ni, key, jcc) : ni;
+        lo[o] = a;
+        cnt[o] = b - a;
+    }
+}
+
+// Output column j of a rule = column src[j] of the concatenation
+// (in0 row ++ in1 row[jcc..]) for a join (as_all_to_allv_{left,right}_join_buffer_helper,
+// shmap_relation_exp.cpp:335-349, 403-417), or of the input row for a copy.
+struct WideProj {
+    int n;        // output columns
+    int left;     // join: the outer rows are in0's (LEFT) or in1's (RIGHT)
+    int W0, W1;   // join: in0 and in1 row widths (arity + 1)
+    int jcc;
+    int src[kWideMaxCols];
+};
+
+// Candidate c: outer row o = last row whose offset is <= c, its (c - off[o])-th match.
+__global__ void __launch_bounds__(kThreads) wide_join_expand_kernel(const u64* __restrict__ outer,
+                                                                    const u64* __restrict__ inner, u64 no,
+                                                                    const u64* __restrict__ lo,
+                                                                    const u64* __restrict__ off, u64 total,
+                                                                    WideProj pj, u64* __restrict__ out)
+{
+    const int Wo = pj.left ? pj.W0 : pj.W1, Wi = pj.left ? pj.W1 : pj.W0;
+    for (u64 c = (u64)blockIdx.x * kThreads + threadIdx.x; c < total; c += (u64)gridDim.x * kThreads) {
+        u64 a = 0, b = no;   // upper_bound over the offsets
+        while (a < b) {
+            const u64 m = (a + b) >> 1;
+            if (off[m] <= c) a = m + 1;
+            else b = m;
+        }
+        const u64 o = a - 1, u = lo[o] + (c - off[o]);
+        const u64* ro = outer + o * (u64)Wo;
+        const u64* ri = inner + u * (u64)Wi;
+        const u64* r0 = pj.left ? ro : ri;
+        const u64* r1 = pj.left ? ri : ro;
+        u64* dst = out + c * (u64)pj.n;
+        for (int j = 0; j < pj.n; j++) {
+            const int x = pj.src[j];
+            dst[j] = x < pj.W0 ? r0[x] : r1[pj.jcc + (x - pj.W0)];
+        }
+    }
+}
+
+// copy_filter's predicate on columns 0 and 1 of each input row.
+__global__ void __launch_bounds__(kThreads) wide_filter_kernel(const u64* __restrict__ in, int Wi, u64 n, int pred,
+                                                               u32* __restrict__ keep)
+{
+    for (u64 r = (u64)blockIdx.x * kThreads + threadIdx.x; r < n; r += (u64)gridDim.x * kThreads) {
+        const u64* row = in + r * (u64)Wi;
+        keep[r] = eval_pred(pred, row[0], Wi > 1 ? row[1] : 0) ? 1u : 0u;
+    }
+}
+
+// copy / acopy / copy_filter (shmap_relation_exp.cpp:116-265): one candidate per
+// input row in trie order; with `keep`, only kept rows, at their scanned positions.
+__global__ void __launch_bounds__(kThreads) wide_copy_kernel(const u64* __restrict__ in, int Wi, u64 n, WideProj pj,
+                                                             const u32* __restrict__ keep, const u64* __restrict__ pos,
+                                                             u64* __restrict__ out)
+{
+    for (u64 r = (u64)blockIdx.x * kThreads + threadIdx.x; r < n; r += (u64)gridDim.x * kThreads) {
+        if (keep && !keep[r]) continue;
+        const u64* row = in + r * (u64)Wi;
+        u64* dst = out + (keep ? pos[r] : r) * (u64)pj.n;
+        for (int j = 0; j < pj.n; j++) dst[j] = row[pj.src[j]];
+    }
+}
+
+// Winners of one relation's candidates (RAM::local_insert_in_newt,
+// src/RAM/RA_tasks.cpp:824-905): in (data columns, position) order, the first
+// of each group of equal candidates wins unless full or delta holds its data
+// columns; later rules' duplicates of earlier rules' winners lose, as against newt.
+__global__ void __launch_bounds__(kThreads) wide_winner_kernel(const u64* __restrict__ cand, int cw,
+                                                               const u64* __restrict__ idx, u64 n,
+                                                               const u64* __restrict__ full, u64 nf,
+                                                               const u64* __restrict__ delta, u64 nd, int W,
+                                                               u32* __restrict__ win)
+{
+    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
+        const u64 c = idx[k];
+        const u64* row = cand + c * (u64)cw;
+        bool w = k == 0 || wide_cmp(cand + idx[k - 1] * (u64)cw, row, cw) != 0;
+        if (w) w = !wide_has_prefix(full, W, nf, row, cw) && !wide_has_prefix(delta, W, nd, row, cw);
+        win[c] = w ? 1u : 0u;
+    }
+}
+
+// Up to kWideMaxSegs segments of a relation's candidate buffer, one per rule
+// writing it, with the id base of each (the tag's intern counter when the rule runs).
+struct WideSegs {
+    int n;
+    u64 start[kWideMaxSegs + 1];   // candidate positions; start[n] = total
+    u64 win_base[kWideMaxSegs];    // winners before the segment
+    u64 id_base[kWideMaxSegs];     // (tag << 46) | counter of the segment's first winner
+};
+
+// New tuples into newt rows (arity + 1 columns) in position order; a join or
+// copy winner gets the next id of its rule's segment, an acopy candidate
+// carries its own last column.
+__global__ void __launch_bounds__(kThreads) wide_newt_kernel(const u64* __restrict__ cand, int cw, u64 n,
+                                                             const u32* __restrict__ win, const u64* __restrict__ wpos,
+                                                             WideSegs sg, int W, u64* __restrict__ newt)
+{
+    for (u64 c = (u64)blockIdx.x * kThreads + threadIdx.x; c < n; c += (u64)gridDim.x * kThreads) {
+        if (!win[c]) continue;
+        int q = 0;
+        while (q + 1 < sg.n && c >= sg.start[q + 1]) q++;
+        const u64 at = wpos[c];
+        const u64* src = cand + c * (u64)cw;
+        u64* dst = newt + at * (u64)W;
+        for (int j = 0; j < cw; j++) dst[j] = src[j];
+        if (cw < W) dst[W - 1] = sg.id_base[q] + (at - sg.win_base[q]);
+    }
+}
+
+// Rank merge of two sorted arrays of W-column rows: a row of A goes before equal
+// rows of B, so duplicates land next to each other.
+__global__ void __launch_bounds__(kThreads) wide_merge_rows_kernel(const u64* __restrict__ A, u64 na,
+                                                                   const u64* __restrict__ B, u64 nb, int W,
+                                                                   u64* __restrict__ out)
+{
+    const u64 n = na + nb;
+    for (u64 p = (u64)blockIdx.x * kThreads + threadIdx.x; p < n; p += (u64)gridDim.x * kThreads) {
+        const bool fromA = p < na;
+        const u64 i = fromA ? p : p - na;
+        const u64* row = fromA ? A + i * (u64)W : B + i * (u64)W;
+        const u64 r = fromA ? wide_lower_bound(B, W, nb, row, W) : wide_upper_bound(A, W, na, row, W);
+        u64* dst = out + (i + r) * (u64)W;
+        for (int j = 0; j < W; j++) dst[j] = row[j];
+    }
+}
+
+// Rows equal (all columns) to their predecessor, in a sorted array.
+__global__ void __launch_bounds__(kThreads) wide_dup_kernel(const u64* __restrict__ rows, int W, u64 n,
+                                                            u32* __restrict__ keep, u32* __restrict__ any_dup)
+{
+    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
+        const bool dup = k > 0 && wide_cmp(rows + (k - 1) * (u64)W, rows + k * (u64)W, W) == 0;
+        keep[k] = dup ? 0u : 1u;
+        if (dup) atomicOr(any_dup, 1u);
+    }
+}
+
+// Kept rows to their scanned positions.
+__global__ void __launch_bounds__(kThreads) wide_compact_kernel(const u64* __restrict__ rows, int W, u64 n,
+                                                                const u32* __restrict__ keep,
+                                                                const u64* __restrict__ pos, u64* __restrict__ out)
+{
+    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
+        if (!keep[k]) continue;
+        const u64* src = rows + k * (u64)W;
+        u64* dst = out + pos[k] * (u64)W;
+        for (int j = 0; j < W; j++) dst[j] = src[j];
+    }
+}
+
+// Exclusive-scanned winner counts at each segment's start (the total past the
+// end), i.e. the winners before each rule's candidates.
+__global__ void wide_pick_kernel(const u64* __restrict__ scanned, u64 n, u64 total, WideSegs sg,
+                                 u64* __restrict__ out)
+{
+    const int q = threadIdx.x;
+    if (q <= sg.n) out[q] = sg.start[q] < n ? scanned[sg.start[q]] : total;
+}
+
+// Count and digest of a relation's rows, data columns only (no instances).
+__global__ void __launch_bounds__(kThreads) wide_summary_kernel(const u64* __restrict__ rows, int W, u64 n,
+                                                                u64* __restrict__ acc)
+{
+    u64 d = 0;
+    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads)
+        d += tuple_digest(rows + k * (u64)W, W - 1);
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd((unsigned long long*)&acc[1], (unsigned long long)d);
+}
+
+}  // namespace ra

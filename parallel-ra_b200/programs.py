@@ -77,3 +77,78 @@ def build_sg(p, edge_rows: np.ndarray) -> dict:
 
 
 PROGRAMS = {"tc": build_tc, "sg": build_sg}
+
+
+# ---------------------------------------------------------------------------
+# programs read from a description (the generated analyses of the reference's
+# tests/ directory, e.g. worstcase-110-terms-4-m.cpp; format in oracle/programs.h)
+# ---------------------------------------------------------------------------
+
+PREDICATES = {"true": 0, "false": 1, "eq": 2, "ne": 3, "lt": 4, "gt": 5, "le": 6, "ge": 7}
+COPY_KINDS = {"copy": COPY, "acopy": ACOPY, "filter": COPY_FILTER}
+
+
+def read_description(path: str) -> dict:
+    """Parse a program description into relations, SCCs (add order), members,
+    rules (per SCC, add order), dependencies and the batch size."""
+    d = {"batch": 1, "relations": [], "sccs": [], "members": [], "rules": [], "deps": []}
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if not t or t[0].startswith("#"):
+                continue
+            k = t[0]
+            if k == "batch":
+                d["batch"] = int(t[1])
+            elif k == "rel":
+                d["relations"].append({"jcc": int(t[1]), "canonical": t[2] == "1", "arity": int(t[3]),
+                                       "tag": int(t[4]), "version": FULL if t[5] == "FULL" else DELTA,
+                                       "name": t[6], "file": None if t[7] == "-" else t[7]})
+            elif k == "scc":
+                d["sccs"].append({"fixpoint": t[1] == "1", "id": int(t[2])})
+            elif k == "member":
+                d["members"].append((int(t[1]), int(t[2]), t[3] == "1"))
+            elif k == "join":
+                d["rules"].append({"scc": int(t[1]), "kind": "join", "out": int(t[2]), "in0": int(t[3]),
+                                   "ver0": FULL if t[4] == "FULL" else DELTA, "in1": int(t[5]),
+                                   "ver1": FULL if t[6] == "FULL" else DELTA,
+                                   "proj": [int(x) for x in t[7].split(",")]})
+            elif k == "copy":
+                d["rules"].append({"scc": int(t[1]), "kind": t[2], "out": int(t[3]), "in0": int(t[4]),
+                                   "ver0": FULL if t[5] == "FULL" else DELTA, "pred": t[6],
+                                   "proj": [int(x) for x in t[7].split(",")]})
+            elif k == "dep":
+                d["deps"].append((int(t[1]), int(t[2])))
+    return d
+
+
+def build_described(p, path: str, data_dir: str) -> dict:
+    """Build a described program on ``p`` (engine or oracle), loading each
+    relation's file from ``data_dir``; returns {relation name: handle} and
+    stores the description's batch size under the key ``"__batch__"``."""
+    from . import datagen
+    d = read_description(path)
+    handles = []
+    out = {}
+    for r in d["relations"]:
+        h = p.relation(r["jcc"], r["arity"], r["tag"], r["name"], r["version"])
+        rows = datagen.read_relation(f"{data_dir}/{r['file']}") if r["file"] else _empty(r["arity"])
+        if rows.shape[1] != r["arity"] + 1:
+            raise ValueError(f"{r['name']}: file has {rows.shape[1]} columns, relation {r['arity'] + 1}")
+        p.load_rows(h, rows)
+        handles.append(h)
+        out[r["name"]] = h
+    sccs = [p.scc(s["fixpoint"], s["id"]) for s in d["sccs"]]
+    for s, r, init in d["members"]:
+        p.add_relation(sccs[s], handles[r], init)
+    for ru in d["rules"]:
+        s = sccs[ru["scc"]]
+        if ru["kind"] == "join":
+            p.join(s, handles[ru["out"]], handles[ru["in0"]], ru["ver0"], handles[ru["in1"]], ru["ver1"], ru["proj"])
+        else:
+            p.copy(s, handles[ru["out"]], handles[ru["in0"]], ru["ver0"], ru["proj"], kind=COPY_KINDS[ru["kind"]],
+                   pred=PREDICATES[ru["pred"]] if ru["kind"] == "filter" else 0)
+    for a, b in d["deps"]:
+        p.depend(sccs[a], sccs[b])
+    out["__batch__"] = d["batch"]
+    return out
