@@ -48,6 +48,11 @@ WORKLOADS = {
     # the largest instance class of the batched mix: a dense closure (dense row-closure evaluator)
     "tc-er16384d2": ("tc", "er", (16384, 32768, 7)),
 }
+# the reference's generated analyses, as program descriptions + relation files
+# (tests/golden/<name>/, written from the reference's tests/<name>.cpp): wide tuples
+DESCRIBED = {"worstcase-110-terms-4-m": "0-CFA-style analysis of a generated 110-term program "
+                                        "(60 relations, arity <= 13, 19 SCCs, batch size 10)",
+             "cfa-4-4-64": "k-CFA analysis (37 relations, arity <= 23, joins on 0..16 columns)"}
 OUTPUT = {"tc": "T", "sg": "SG"}
 INPUT = {"tc": "G", "sg": "edge"}
 # bounded CPU samples of the same graph families
@@ -204,6 +209,18 @@ def metric_of(kind):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return None
+    if args.workload in DESCRIBED:
+        vals = [described_reference_run(args.workload) for _ in range(max(1, min(args.steps, 2)))]
+        facts, secs = vals[0][0], sum(v[1] for v in vals) / len(vals)
+        sample = f"the whole program on the reference library, {len(vals)} run(s)"
+        return {"impl": "reference", "metric": "facts/s", "value": facts / secs, "unit": "facts/s",
+                "n_gpus": args.gpus, "steps": len(vals), "warmup": 0, "ms_per_step": 1e3 * secs,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "the reference's own input relations", "config": {"workload": args.workload,
+                                                                           "metric_family": METRIC_FAMILY},
+                "cpu_baseline": {"value": facts / secs, "unit": "facts/s", "cores": 1, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": facts / secs, "unit": "facts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "batched":
         from parallel_ra_b200.batch import estimate_tuples
         insts = batched_instances(BATCH_COUNT, BATCH_SEED)
@@ -372,6 +389,126 @@ def run_ours(args, rank, world, local_rank):
         ctc, csecs, kind = reference_sample_run(prog_kind)
         line["cpu_baseline"] = {"value": ctc / csecs, "unit": "tuples/s", "cores": 1, "kind": kind,
                                 "sample": cpu_sample_desc(prog_kind)}
+    return line
+
+
+def described_paths(name):
+    d = os.path.join(ROOT, "tests", "golden", name)
+    return os.path.join(d, "program.txt"), os.path.join(d, "data")
+
+
+def described_reference_run(name):
+    """The reference library on the described program (oracle/_ref/ref_driver, one
+    core): (total facts, fixpoint seconds = the sum of its execute_in_batches calls)."""
+    import tempfile
+    import parallel_ra_b200 as P
+    prog, data = described_paths(name)
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    with tempfile.TemporaryDirectory() as work:
+        empty = os.path.join(work, "empty")
+        P.datagen.write_empty_relation(empty)
+        out = os.path.join(work, "out")
+        subprocess.run([drv, "file", prog, empty, out, data], check=True, stdout=subprocess.DEVNULL)
+        facts = sum(int(ln.split()[2]) for ln in open(os.path.join(out, "sizes.txt")))
+        secs = float(open(os.path.join(out, "time.txt")).read())
+    return facts, secs
+
+
+def run_described_ours(args, rank, world, local_rank):
+    """A generated analysis on the wide-tuple path: facts/s = all relations' final
+    tuples over the device time of one LIE::execute (relations resident in HBM)."""
+    import torch
+    import parallel_ra_b200 as P
+
+    torch.cuda.set_device(local_rank)
+    prog_path, data = described_paths(args.workload)
+    stream = torch.cuda.Stream()
+    prog = P.Program(local_rank)
+    prog.set_stream(stream.cuda_stream)
+    rels = P.programs.build_described(prog, prog_path, data)
+    batch = rels.pop("__batch__")
+    host_rows = {name: P.datagen.read_relation(os.path.join(data, f)) for name, f in
+                 ((r["name"], r["file"]) for r in P.programs.read_description(prog_path)["relations"]) if f}
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f"cuda:{local_rank}")
+    for _ in range(args.warmup):
+        prog.execute(batch)
+    facts = sum(prog.full_count(h) for h in rels.values())
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches = 0
+    with ClockSampler(local_rank) as clocks:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            starts[i].record(stream)
+            prog.execute(batch)
+            ends[i].record(stream)
+            launches += prog.stats().kernel_launches
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * facts * args.steps / (total_ms / 1e3)
+    st = prog.stats()
+    # device time per phase of the wide iteration (per-launch events, one extra run)
+    prog.set_launch_timing(True)
+    prog.execute(batch)
+    ph = prog.stats().phase_ms
+    prog.set_launch_timing(False)
+    names = ("join ranges + scan", "plan", "candidates (join expand / copy)", "winners (sort + dedup)",
+             "newt (ids + sort)", "full + delta merge")
+    phases = {n: round(v, 3) for n, v in zip(names, ph) if n != "plan"}
+    # end to end through the C ABI: every relation from pinned host rows, then history + counts back
+    pinned = {n: torch.from_numpy(r.view(np.int64)).pin_memory().numpy().view(np.uint64) for n, r in host_rows.items()}
+    e2e_s = []
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for n, r in pinned.items():
+            prog.load_rows(rels[n], r)
+        prog.execute(batch)
+        hist = prog.history()
+        got = sum(prog.full_count(h) for h in rels.values())
+        e2e_s.append(time.perf_counter() - t0)
+        assert got == facts
+    h2d = int(sum(r.nbytes for r in host_rows.values()))
+    d2h = 8 * (2 * len(rels) + sum(2 + 2 * len(x[1]) for x in hist))
+    e2e = {"value": facts / statistics.mean(e2e_s), "unit": "facts/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": int(d2h)}
+    peak, peak_kind = load_peaks()
+    dom = max(phases, key=phases.get)
+    if rank != 0:
+        return None
+    line = {
+        "metric": "facts/s", "value": value, "unit": "facts/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "the reference's own input relations (tests/golden fixtures)",
+        "config": {"workload": args.workload, "program": DESCRIBED[args.workload], "batch_size": batch,
+                   "output_facts": facts, "iterations": int(st.iterations), "join_candidates": int(st.join_candidates),
+                   "path": "wide tuples (rows of u64 columns, trie order)",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "phase_ms_per_run": phases, "parallelism": f"{world} independent instance(s), one per GPU",
+                   "metric_family": METRIC_FAMILY},
+        "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": int(launches),
+        "roofline": {"kernel": dom, "bound": "latency", "achieved": None, "peak": peak, "unit": "GB/s",
+                     "frac": None, "peak_kind": peak_kind, "traffic": None,
+                     "note": f"{int(st.kernel_launches)} launches per run over {int(st.iterations)} iterations of "
+                             f"small deltas: launch- and synchronisation-bound, not HBM-bound"},
+        "step_ms": step_ms,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rf, rs = described_reference_run(args.workload)
+        assert rf == facts
+        line["cpu_baseline"] = {"value": rf / rs, "unit": "facts/s", "cores": 1, "kind": "reference",
+                                "sample": f"the whole program on the reference library (fixpoint {rs:.1f} s)"}
     return line
 
 
@@ -651,7 +788,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tc-er22", choices=sorted(WORKLOADS) + ["batched", "served"])
+    ap.add_argument("--workload", default="tc-er22",
+                    choices=sorted(WORKLOADS) + sorted(DESCRIBED) + ["batched", "served"])
     ap.add_argument("--slots", type=int, default=4, help="served: concurrent waves (worker threads)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="served: device-memory admission budget")
     ap.add_argument("--wave-tuples", type=float, default=0.0,
@@ -677,6 +815,11 @@ def main():
         line = run_batched(args, rank, world, local_rank)
     elif args.workload == "served":
         line = run_served(args, rank, world, local_rank)
+    elif args.workload in DESCRIBED:
+        line = run_described_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
     else:
         line = run_ours(args, rank, world, local_rank)
         if world > 1:

@@ -9,6 +9,7 @@ Run ``python parallel-ra_b200/build.py``; it is also what
 """
 from __future__ import annotations
 
+import glob
 import os
 import subprocess
 import sys
@@ -19,8 +20,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 ENGINE_SRCS = [os.path.join(HERE, "csrc", "ra_engine.cu")]   # includes csrc/ra_noalloc.cu
-ENGINE_DEPS = ENGINE_SRCS + [os.path.join(HERE, "csrc", f) for f in (
-    "ra_device.cuh", "ra_kernels.cuh", "ra_iter.cuh", "ra_dense.cuh", "ra_noalloc.cu")] + [
+# every source of the engine's single translation unit (ra_engine.cu includes the rest)
+ENGINE_DEPS = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
     os.path.join(ROOT, "include", "ra_engine.h")]
 ENGINE_LIB = os.path.join(HERE, "libra_b200.so")
 

@@ -23,7 +23,7 @@
 // (Included inside the engine's anonymous namespace.)
 
 // Scratch slots of the wide path (grow-only, contents not kept across calls).
-enum WideSlot { kWsIdxA, kWsIdxB, kWsRows, kWsLo, kWsCnt, kWsOff, kWsPos, kWsFlag, kWsSmall, kWsCount };
+enum WideSlot { kWsIdxA, kWsIdxB, kWsRows, kWsLo, kWsCnt, kWsOff, kWsPos, kWsFlag, kWsSmall, kWsTot, kWsCount };
 static_assert(kWsCount <= 12, "wide scratch slots");
 
 u64* wide_scratch(ra_program* p, int slot, u64 n)
@@ -67,14 +67,34 @@ void wide_reserve32(ra_program* p, u32** buf, u64* cap, u64 n)
 
 int wide_grid(u64 n) { return grid_for(std::max<u64>(n, 1)); }
 
+// Exclusive scan of n values into out, the total into *total_dev, with no host
+// round trip (one block for small inputs).
+template <typename T>
+void wide_scan_async(ra_program* p, const T* in, u64 n, u64* out, u64* total_dev)
+{
+    if (n <= (u64)kThreads * kWideScanPer) {
+        wide_scan_small_kernel<T><<<1, kThreads, 0, p->stream>>>(in, n, out, total_dev);
+        LAUNCHED();
+        return;
+    }
+    scan_exclusive<T>(p, in, n, out, false);
+    CK(cudaMemcpyAsync(total_dev, p->dscalar, 8, cudaMemcpyDeviceToDevice, p->stream));
+}
+
 // Indices 0..n-1 of `rows` sorted by (first ncmp columns, index); the result is
 // one of the two index scratch slots.
 const u64* wide_sort(ra_program* p, const u64* rows, int W, int ncmp, u64 n)
 {
     u64* a = wide_scratch(p, kWsIdxA, n);
     u64* b = wide_scratch(p, kWsIdxB, n);
-    const u64 tiles = (n + kWideSortTile - 1) / kWideSortTile;
-    wide_tile_sort_kernel<<<(unsigned)tiles, kThreads, 0, p->stream>>>(rows, W, ncmp, n, a);
+    if (n <= 64) {
+        wide_tile_sort_kernel<64><<<1, kThreads, 0, p->stream>>>(rows, W, ncmp, n, a);
+    } else if (n <= 256) {
+        wide_tile_sort_kernel<256><<<1, kThreads, 0, p->stream>>>(rows, W, ncmp, n, a);
+    } else {
+        const u64 tiles = (n + kWideSortTile - 1) / kWideSortTile;
+        wide_tile_sort_kernel<kWideSortTile><<<(unsigned)tiles, kThreads, 0, p->stream>>>(rows, W, ncmp, n, a);
+    }
     LAUNCHED();
     for (u64 L = kWideSortTile; L < n; L *= 2) {
         wide_merge_pass_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(rows, W, ncmp, n, L, a, b);
@@ -215,157 +235,245 @@ WideProj wide_proj(ra_program* p, const Scc& s, const Rule& ru, int cw)
 struct WideOut {
     int rel;
     int cw;
-    u64 n = 0;                      // candidates so far
+    u64 n = 0;                      // candidates
     std::vector<int> rules;         // rule index of each segment
     std::vector<u64> seg_start;     // first candidate of each segment
     u64 winners = 0;
     std::vector<u64> seg_wins;      // winners before each segment, then the total
 };
 
-// One iteration: RAM::local_compute + local_insert_in_newt + local_insert_in_full.
+// Inputs of one rule in the running iteration.
+struct WideRuleRun {
+    bool active = false;
+    const u64* outer = nullptr;     // join: outer rows; copy: input rows
+    const u64* inner = nullptr;
+    u64 no = 0, ni = 0;             // join: outer / inner rows; copy: input rows in `no`
+    u64 off = 0;                    // this rule's region of the per-rule scratch
+    WideProj pj{};
+    u64 total = 0;                  // candidates
+};
+
+// One iteration: RAM::local_compute + local_insert_in_newt + local_insert_in_full,
+// with two host round trips: after the candidate counts, and after the winners.
 void wide_iteration(ra_program* p, Scc& s)
 {
+    const int nr = (int)s.rules.size();
     std::vector<WideOut> outs;
     outs.reserve(s.rules.size());
-    auto out_of = [&](int rel) -> WideOut& {
-        for (WideOut& o : outs)
-            if (o.rel == rel) return o;
-        WideOut o;
-        o.rel = rel;
-        o.cw = wide_cand_width(p, s, rel);
-        Relation& R = p->rels[rel];
-        if (R.wcand_w != o.cw) {   // the buffer's capacity counts rows of its last width
-            dev_free(p, &R.wcand);
-            R.wcand_cap = 0;
-            R.wcand_w = o.cw;
+    std::vector<int> out_index(nr);
+    for (int q = 0; q < nr; q++) {
+        const int rel = s.rules[q].out;
+        int k = 0;
+        while (k < (int)outs.size() && outs[k].rel != rel) k++;
+        if (k == (int)outs.size()) {
+            WideOut o;
+            o.rel = rel;
+            o.cw = wide_cand_width(p, s, rel);
+            Relation& R = p->rels[rel];
+            if (R.wcand_w != o.cw) {   // the buffer's capacity counts rows of its last width
+                dev_free(p, &R.wcand);
+                R.wcand_cap = 0;
+                R.wcand_w = o.cw;
+            }
+            outs.push_back(o);
         }
-        outs.push_back(o);
-        return outs.back();
-    };
-    // 1. candidates, rule by rule
-    for (size_t q = 0; q < s.rules.size(); q++) {
-        const Rule& ru = s.rules[q];
-        WideOut& wo = out_of(ru.out);
-        Relation& R = p->rels[ru.out];
-        const WideProj pj = wide_proj(p, s, ru, wo.cw);
-        if ((int)wo.rules.size() >= kWideMaxSegs)
+        out_index[q] = k;
+        if ((int)outs[k].rules.size() >= kWideMaxSegs)
             fail(p, RA_E_UNSUPPORTED, "SCC %d: more than %d rules write relation %s", s.id, kWideMaxSegs,
-                 R.name.c_str());
-        wo.rules.push_back((int)q);
-        wo.seg_start.push_back(wo.n);
+                 p->rels[rel].name.c_str());
+        outs[k].rules.push_back(q);
+    }
+    // inputs of every rule
+    std::vector<WideRuleRun> rr(nr);
+    u64 join_rows = 0, filter_rows = 0;
+    for (int q = 0; q < nr; q++) {
+        const Rule& ru = s.rules[q];
+        WideRuleRun& r = rr[q];
+        r.pj = wide_proj(p, s, ru, outs[out_index[q]].cw);
+        Relation& a = p->rels[ru.in0];
         if (ru.kind == kJoin) {
-            Relation& a = p->rels[ru.in0];
             Relation& b = p->rels[ru.in1];
-            u64 no, ni;
-            const u64 *outer, *inner;
             if (ru.ver0 == RA_DELTA) {
-                outer = wide_version(a, RA_DELTA, &no);
-                inner = wide_version(b, ru.ver1, &ni);
+                r.outer = wide_version(a, RA_DELTA, &r.no);
+                r.inner = wide_version(b, ru.ver1, &r.ni);
             } else {
-                outer = wide_version(b, ru.ver1, &no);
-                inner = wide_version(a, RA_FULL, &ni);
+                r.outer = wide_version(b, ru.ver1, &r.no);
+                r.inner = wide_version(a, RA_FULL, &r.ni);
             }
-            if (!no || !ni) continue;
-            u64* lo = wide_scratch(p, kWsLo, no);
-            u64* cnt = wide_scratch(p, kWsCnt, no);
-            u64* off = wide_scratch(p, kWsOff, no);
-            const int Wo = pj.left ? pj.W0 : pj.W1, Wi = pj.left ? pj.W1 : pj.W0;
-            wide_join_count_kernel<<<wide_grid(no), kThreads, 0, p->stream>>>(outer, Wo, no, inner, Wi, ni, pj.jcc, lo,
-                                                                              cnt);
-            LAUNCHED();
-            const u64 total = scan_exclusive<u64>(p, cnt, no, off);
-            if (!total) continue;
-            wide_reserve(p, &R.wcand, &R.wcand_cap, wo.n + total, wo.cw, wo.n);
-            wide_join_expand_kernel<<<wide_grid(total), kThreads, 0, p->stream>>>(
-                outer, inner, no, lo, off, total, pj, R.wcand + wo.n * (u64)wo.cw);
-            LAUNCHED();
-            wo.n += total;
-            p->stats.join_candidates += total;
+            r.active = r.no && r.ni;
+            if (r.active) {
+                r.off = join_rows;
+                join_rows += r.no;
+            }
         } else {
-            Relation& a = p->rels[ru.in0];
-            u64 n;
-            const u64* in = wide_version(a, ru.ver0, &n);
-            if (!n) continue;
-            const int Wi = (int)a.arity + 1;
-            u64 m = n;
-            u32* keep = nullptr;
-            u64* pos = nullptr;
-            if (ru.kind == RA_COPY_FILTER) {
-                keep = wide_scratch32(p, kWsFlag, n);
-                pos = wide_scratch(p, kWsPos, n);
-                wide_filter_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(in, Wi, n, ru.pred, keep);
-                LAUNCHED();
-                m = scan_exclusive<u32>(p, keep, n, pos);
-                if (!m) continue;
+            r.outer = wide_version(a, ru.ver0, &r.no);
+            r.active = r.no != 0;
+            r.total = r.no;
+            if (r.active && ru.kind == RA_COPY_FILTER) {
+                r.off = filter_rows;
+                filter_rows += r.no;
             }
-            wide_reserve(p, &R.wcand, &R.wcand_cap, wo.n + m, wo.cw, wo.n);
-            wide_copy_kernel<<<wide_grid(n), kThreads, 0, p->stream>>>(in, Wi, n, pj, keep, pos,
-                                                                       R.wcand + wo.n * (u64)wo.cw);
-            LAUNCHED();
-            wo.n += m;
         }
     }
-    // 2. winners per output relation
-    for (WideOut& wo : outs) {
-        Relation& R = p->rels[wo.rel];
-        wo.seg_wins.assign(wo.rules.size() + 1, 0);
-        if (!wo.n) continue;
-        const int W = (int)R.arity + 1;
-        const u64* idx = wide_sort(p, R.wcand, wo.cw, wo.cw, wo.n);
-        wide_reserve32(p, &R.wflag, &R.wflag_cap, wo.n);
-        wide_reserve(p, &R.wpos, &R.wpos_cap, wo.n, 1, 0);
-        wide_winner_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, idx, wo.n, R.wfull, R.full_n,
-                                                                        R.wdelta, R.delta_n, W, R.wflag);
-        LAUNCHED();
-        wo.winners = scan_exclusive<u32>(p, R.wflag, wo.n, R.wpos);
-        WideSegs sg{};
-        sg.n = (int)wo.rules.size();
-        for (int k = 0; k < sg.n; k++) sg.start[k] = wo.seg_start[k];
-        sg.start[sg.n] = wo.n;
-        u64* small = wide_scratch(p, kWsSmall, kWideMaxSegs + 1);
-        wide_pick_kernel<<<1, kWideMaxSegs + 1, 0, p->stream>>>(R.wpos, wo.n, wo.winners, sg, small);
-        LAUNCHED();
-        CK(cudaMemcpyAsync(wo.seg_wins.data(), small, (sg.n + 1) * 8, cudaMemcpyDeviceToHost, p->stream));
-        CK(cudaStreamSynchronize(p->stream));
-        // the newt rows need the ids of every relation's earlier rules: after all relations
-        R.newt_n = wo.winners;
-        if (wo.winners) wide_reserve(p, &R.wnewt, &R.wnewt_cap, wo.winners, W, 0);
+    // 1. candidate counts (join ranges, filter passes), one round trip for all rules
+    u64* tot = wide_scratch(p, kWsTot, (u64)nr + outs.size() * (kWideMaxSegs + 2));
+    u64* lo = join_rows ? wide_scratch(p, kWsLo, join_rows) : nullptr;
+    u64* cnt = join_rows ? wide_scratch(p, kWsCnt, join_rows) : nullptr;
+    u64* off = join_rows ? wide_scratch(p, kWsOff, join_rows) : nullptr;
+    u32* keep = filter_rows ? wide_scratch32(p, kWsFlag, filter_rows) : nullptr;
+    u64* pos = filter_rows ? wide_scratch(p, kWsPos, filter_rows) : nullptr;
+    bool counted = false;
+    {
+        PhaseTimer pt(p, 0);
+        for (int q = 0; q < nr; q++) {
+            const Rule& ru = s.rules[q];
+            WideRuleRun& r = rr[q];
+            if (!r.active) continue;
+            if (ru.kind == kJoin) {
+                const int Wo = r.pj.left ? r.pj.W0 : r.pj.W1, Wi = r.pj.left ? r.pj.W1 : r.pj.W0;
+                wide_join_count_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wo, r.no, r.inner, Wi,
+                                                                                    r.ni, r.pj.jcc, lo + r.off,
+                                                                                    cnt + r.off);
+                LAUNCHED();
+                wide_scan_async<u64>(p, cnt + r.off, r.no, off + r.off, tot + q);
+                counted = true;
+            } else if (ru.kind == RA_COPY_FILTER) {
+                const int Wi = (int)p->rels[ru.in0].arity + 1;
+                wide_filter_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wi, r.no, ru.pred,
+                                                                                keep + r.off);
+                LAUNCHED();
+                wide_scan_async<u32>(p, keep + r.off, r.no, pos + r.off, tot + q);
+                counted = true;
+            }
+        }
+        if (counted) {
+            std::vector<u64> h(nr);
+            CK(cudaMemcpyAsync(h.data(), tot, nr * 8, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+            for (int q = 0; q < nr; q++)
+                if (rr[q].active && (s.rules[q].kind == kJoin || s.rules[q].kind == RA_COPY_FILTER)) rr[q].total = h[q];
+        }
     }
-    // 3. ids: rule by rule in the SCC's order, each tag's counter shared by its relations
-    std::vector<u64> id_base(s.rules.size(), 0);
-    for (size_t q = 0; q < s.rules.size(); q++) {
+    // 2. candidates into each output relation's buffer, rule by rule
+    {
+        PhaseTimer pt(p, 2);
+        for (WideOut& wo : outs) {
+            Relation& R = p->rels[wo.rel];
+            wo.n = 0;
+            for (int q : wo.rules) {
+                wo.seg_start.push_back(wo.n);
+                if (rr[q].active) wo.n += rr[q].total;
+            }
+            if (wo.n) wide_reserve(p, &R.wcand, &R.wcand_cap, wo.n, wo.cw, 0);
+            for (size_t k = 0; k < wo.rules.size(); k++) {
+                const int q = wo.rules[k];
+                const Rule& ru = s.rules[q];
+                WideRuleRun& r = rr[q];
+                if (!r.active || !r.total) continue;
+                u64* dst = R.wcand + wo.seg_start[k] * (u64)wo.cw;
+                if (ru.kind == kJoin) {
+                    wide_join_expand_kernel<<<wide_grid(r.total), kThreads, 0, p->stream>>>(
+                        r.outer, r.inner, r.no, lo + r.off, off + r.off, r.total, r.pj, dst);
+                    p->stats.join_candidates += r.total;
+                } else {
+                    const int Wi = (int)p->rels[ru.in0].arity + 1;
+                    const bool f = ru.kind == RA_COPY_FILTER;
+                    wide_copy_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wi, r.no, r.pj,
+                                                                                 f ? keep + r.off : nullptr,
+                                                                                 f ? pos + r.off : nullptr, dst);
+                }
+                LAUNCHED();
+            }
+        }
+    }
+    // 3. winners of every output relation, one round trip for all of them
+    u64* picks = tot + nr;   // per relation: kWideMaxSegs + 1 picked counts, then its winner total
+    bool any = false;
+    {
+        PhaseTimer pt(p, 3);
+        for (size_t k = 0; k < outs.size(); k++) {
+            WideOut& wo = outs[k];
+            Relation& R = p->rels[wo.rel];
+            if (!wo.n) continue;
+            any = true;
+            const int W = (int)R.arity + 1;
+            const u64* idx = wide_sort(p, R.wcand, wo.cw, wo.cw, wo.n);
+            wide_reserve32(p, &R.wflag, &R.wflag_cap, wo.n);
+            wide_reserve(p, &R.wpos, &R.wpos_cap, wo.n, 1, 0);
+            wide_winner_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, idx, wo.n, R.wfull,
+                                                                            R.full_n, R.wdelta, R.delta_n, W, R.wflag);
+            LAUNCHED();
+            u64* my = picks + k * (kWideMaxSegs + 2);
+            wide_scan_async<u32>(p, R.wflag, wo.n, R.wpos, my + kWideMaxSegs + 1);
+            WideSegs sg{};
+            sg.n = (int)wo.rules.size();
+            for (int j = 0; j < sg.n; j++) sg.start[j] = wo.seg_start[j];
+            sg.start[sg.n] = wo.n;
+            wide_pick_kernel<<<1, kWideMaxSegs + 1, 0, p->stream>>>(R.wpos, wo.n, my + kWideMaxSegs + 1, sg, my);
+            LAUNCHED();
+        }
+        std::vector<u64> h(outs.size() * (kWideMaxSegs + 2));
+        if (any) {
+            CK(cudaMemcpyAsync(h.data(), picks, h.size() * 8, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+        }
+        for (size_t k = 0; k < outs.size(); k++) {
+            WideOut& wo = outs[k];
+            Relation& R = p->rels[wo.rel];
+            wo.seg_wins.assign(wo.rules.size() + 1, 0);
+            if (wo.n) {
+                const u64* my = h.data() + k * (kWideMaxSegs + 2);
+                for (size_t j = 0; j <= wo.rules.size(); j++) wo.seg_wins[j] = my[j];
+                wo.winners = my[kWideMaxSegs + 1];
+            }
+            R.newt_n = wo.winners;
+            if (wo.winners) wide_reserve(p, &R.wnewt, &R.wnewt_cap, wo.winners, (int)R.arity + 1, 0);
+        }
+    }
+    // 4. ids: rule by rule in the SCC's order, each tag's counter shared by its relations
+    std::vector<u64> id_base(nr, 0);
+    for (int q = 0; q < nr; q++) {
         const Rule& ru = s.rules[q];
         if (ru.kind == RA_ACOPY) continue;
-        WideOut& wo = out_of(ru.out);
-        const size_t k = std::find(wo.rules.begin(), wo.rules.end(), (int)q) - wo.rules.begin();
+        WideOut& wo = outs[out_index[q]];
+        const size_t k = std::find(wo.rules.begin(), wo.rules.end(), q) - wo.rules.begin();
         const u64 wins = wo.seg_wins[k + 1] - wo.seg_wins[k];
         u64& ctr = intern_counter(p, p->rels[ru.out].tag);
         id_base[q] = ((u64)p->rels[ru.out].tag << 46) | ctr;
         ctr += wins;
     }
-    // 4. newt rows, sorted into trie order
-    for (WideOut& wo : outs) {
-        Relation& R = p->rels[wo.rel];
-        if (!wo.winners) continue;
-        const int W = (int)R.arity + 1;
-        WideSegs sg{};
-        sg.n = (int)wo.rules.size();
-        for (int k = 0; k < sg.n; k++) {
-            sg.start[k] = wo.seg_start[k];
-            sg.win_base[k] = wo.seg_wins[k];
-            sg.id_base[k] = id_base[wo.rules[k]];
+    // 5. newt rows, sorted into trie order
+    {
+        PhaseTimer pt(p, 4);
+        for (WideOut& wo : outs) {
+            Relation& R = p->rels[wo.rel];
+            if (!wo.winners) continue;
+            const int W = (int)R.arity + 1;
+            WideSegs sg{};
+            sg.n = (int)wo.rules.size();
+            for (int k = 0; k < sg.n; k++) {
+                sg.start[k] = wo.seg_start[k];
+                sg.win_base[k] = wo.seg_wins[k];
+                sg.id_base[k] = id_base[wo.rules[k]];
+            }
+            sg.start[sg.n] = wo.n;
+            u64* rows = wide_scratch(p, kWsRows, wo.winners * (u64)W);
+            wide_newt_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, wo.n, R.wflag, R.wpos, sg,
+                                                                           W, rows);
+            LAUNCHED();
+            if (wo.winners == 1) {
+                CK(cudaMemcpyAsync(R.wnewt, rows, (u64)W * 8, cudaMemcpyDeviceToDevice, p->stream));
+            } else {
+                const u64* idx = wide_sort(p, rows, W, W, wo.winners);
+                wide_gather_kernel<<<wide_grid(wo.winners * W), kThreads, 0, p->stream>>>(rows, W, idx, wo.winners,
+                                                                                         R.wnewt);
+                LAUNCHED();
+            }
+            p->stats.new_tuples += wo.winners;
         }
-        sg.start[sg.n] = wo.n;
-        u64* rows = wide_scratch(p, kWsRows, wo.winners * (u64)W);
-        wide_newt_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, wo.n, R.wflag, R.wpos, sg, W,
-                                                                       rows);
-        LAUNCHED();
-        const u64* idx = wide_sort(p, rows, W, W, wo.winners);
-        wide_gather_kernel<<<wide_grid(wo.winners * W), kThreads, 0, p->stream>>>(rows, W, idx, wo.winners, R.wnewt);
-        LAUNCHED();
-        p->stats.new_tuples += wo.winners;
     }
     // local_insert_in_full: full = full + delta, delta = newt
+    PhaseTimer pt(p, 5);
     for (int ri : s.rels) {
         Relation& R = p->rels[ri];
         wide_delta_to_full(p, R);

@@ -36,21 +36,23 @@ __device__ __forceinline__ bool wide_before(const u64* __restrict__ rows, int W,
     return c < 0 || (c == 0 && i < j);
 }
 
-// Tile sort: indices [tile * kWideSortTile, ...) of `n` rows, bitonic network in
-// shared memory (missing entries are a sentinel that orders last).
+// Tile sort: indices [tile * TILE, ...) of `n` rows, bitonic network in shared
+// memory (missing entries are a sentinel that orders last).  Small inputs take
+// a small tile: the network's depth grows with log^2 of the tile.
+template <int TILE>
 __global__ void __launch_bounds__(kThreads) wide_tile_sort_kernel(const u64* __restrict__ rows, int W, int ncmp,
                                                                   u64 n, u64* __restrict__ idx)
 {
-    __shared__ u64 s[kWideSortTile];
-    const u64 base = (u64)blockIdx.x * kWideSortTile;
-    for (int t = threadIdx.x; t < kWideSortTile; t += kThreads) {
+    __shared__ u64 s[TILE];
+    const u64 base = (u64)blockIdx.x * TILE;
+    for (int t = threadIdx.x; t < TILE; t += kThreads) {
         const u64 g = base + t;
         s[t] = g < n ? g : ~0ull;
     }
     __syncthreads();
-    for (int k = 2; k <= kWideSortTile; k <<= 1) {
+    for (int k = 2; k <= TILE; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int t = threadIdx.x; t < kWideSortTile; t += kThreads) {
+            for (int t = threadIdx.x; t < TILE; t += kThreads) {
                 const int partner = t ^ j;
                 if (partner <= t) continue;
                 const u64 a = s[t], b = s[partner];
@@ -66,10 +68,32 @@ __global__ void __launch_bounds__(kThreads) wide_tile_sort_kernel(const u64* __r
             __syncthreads();
         }
     }
-    for (int t = threadIdx.x; t < kWideSortTile; t += kThreads) {
+    for (int t = threadIdx.x; t < TILE; t += kThreads) {
         const u64 g = base + t;
         if (g < n) idx[g] = s[t];
     }
+}
+
+// Exclusive scan of at most kThreads * kWideScanPer values by one block; the
+// total into *total (device memory: no host round trip).
+constexpr int kWideScanPer = 16;
+template <typename T>
+__global__ void __launch_bounds__(kThreads) wide_scan_small_kernel(const T* __restrict__ in, u64 n,
+                                                                   u64* __restrict__ out, u64* __restrict__ total)
+{
+    __shared__ u64 sm[kWarps + 1];
+    const u64 base = (u64)threadIdx.x * kWideScanPer;
+    u64 loc = 0;
+    for (int k = 0; k < kWideScanPer; k++)
+        if (base + k < n) loc += (u64)in[base + k];
+    u64 agg;
+    u64 ex = block_exclusive_scan(loc, sm, &agg);
+    for (int k = 0; k < kWideScanPer; k++)
+        if (base + k < n) {
+            out[base + k] = ex;
+            ex += (u64)in[base + k];
+        }
+    if (threadIdx.x == 0) *total = agg;
 }
 
 // One merge pass: sorted runs of length L in `in`, pairs merged into `out`.  An
@@ -323,11 +347,11 @@ __global__ void __launch_bounds__(kThreads) wide_compact_kernel(const u64* __res
 
 // Exclusive-scanned winner counts at each segment's start (the total past the
 // end), i.e. the winners before each rule's candidates.
-__global__ void wide_pick_kernel(const u64* __restrict__ scanned, u64 n, u64 total, WideSegs sg,
-                                 u64* __restrict__ out)
+__global__ void wide_pick_kernel(const u64* __restrict__ scanned, u64 n, const u64* __restrict__ total,
+                                 WideSegs sg, u64* __restrict__ out)
 {
     const int q = threadIdx.x;
-    if (q <= sg.n) out[q] = sg.start[q] < n ? scanned[sg.start[q]] : total;
+    if (q <= sg.n) out[q] = sg.start[q] < n ? scanned[sg.start[q]] : *total;
 }
 
 // Count and digest of a relation's rows, data columns only (no instances).
