@@ -325,27 +325,42 @@ void wide_iteration(ra_program* p, Scc& s)
     bool counted = false;
     {
         PhaseTimer pt(p, 0);
+        WideCountBatch cb{};
+        auto flush_counts = [&]() {
+            if (!cb.n) return;
+            wide_count_batch_kernel<<<cb.n, kThreads, 0, p->stream>>>(cb);
+            LAUNCHED();
+            cb.n = 0;
+        };
         for (int q = 0; q < nr; q++) {
             const Rule& ru = s.rules[q];
             WideRuleRun& r = rr[q];
-            if (!r.active) continue;
-            if (ru.kind == kJoin) {
-                const int Wo = r.pj.left ? r.pj.W0 : r.pj.W1, Wi = r.pj.left ? r.pj.W1 : r.pj.W0;
+            if (!r.active || (ru.kind != kJoin && ru.kind != RA_COPY_FILTER)) continue;
+            counted = true;
+            const bool join = ru.kind == kJoin;
+            const int Wo = join ? (r.pj.left ? r.pj.W0 : r.pj.W1) : (int)p->rels[ru.in0].arity + 1;
+            const int Wi = join ? (r.pj.left ? r.pj.W1 : r.pj.W0) : 0;
+            if (r.no <= kWideBlockScan) {   // small: one block of the batched launch
+                WideCountJob& j = cb.job[cb.n++];
+                j = WideCountJob{r.outer, r.inner, r.no, r.ni, join ? lo + r.off : nullptr,
+                                 join ? cnt + r.off : nullptr, join ? off + r.off : pos + r.off,
+                                 join ? nullptr : keep + r.off, tot + q, Wo, Wi, join ? r.pj.jcc : 0,
+                                 join ? -1 : ru.pred};
+                if (cb.n == kWideJobs) flush_counts();
+            } else if (join) {
                 wide_join_count_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wo, r.no, r.inner, Wi,
                                                                                     r.ni, r.pj.jcc, lo + r.off,
                                                                                     cnt + r.off);
                 LAUNCHED();
                 wide_scan_async<u64>(p, cnt + r.off, r.no, off + r.off, tot + q);
-                counted = true;
-            } else if (ru.kind == RA_COPY_FILTER) {
-                const int Wi = (int)p->rels[ru.in0].arity + 1;
-                wide_filter_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wi, r.no, ru.pred,
+            } else {
+                wide_filter_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wo, r.no, ru.pred,
                                                                                 keep + r.off);
                 LAUNCHED();
                 wide_scan_async<u32>(p, keep + r.off, r.no, pos + r.off, tot + q);
-                counted = true;
             }
         }
+        flush_counts();
         if (counted) {
             std::vector<u64> h(nr);
             CK(cudaMemcpyAsync(h.data(), tot, nr * 8, cudaMemcpyDeviceToHost, p->stream));
@@ -354,9 +369,17 @@ void wide_iteration(ra_program* p, Scc& s)
                 if (rr[q].active && (s.rules[q].kind == kJoin || s.rules[q].kind == RA_COPY_FILTER)) rr[q].total = h[q];
         }
     }
-    // 2. candidates into each output relation's buffer, rule by rule
+    // 2. candidates into each output relation's buffer, rule by rule, one flattened launch
     {
         PhaseTimer pt(p, 2);
+        WideExpandBatch eb{};
+        auto flush_expand = [&]() {
+            if (!eb.n) return;
+            wide_expand_batch_kernel<<<wide_grid(eb.total), kThreads, 0, p->stream>>>(eb);
+            LAUNCHED();
+            eb.n = 0;
+            eb.total = 0;
+        };
         for (WideOut& wo : outs) {
             Relation& R = p->rels[wo.rel];
             wo.n = 0;
@@ -365,53 +388,90 @@ void wide_iteration(ra_program* p, Scc& s)
                 if (rr[q].active) wo.n += rr[q].total;
             }
             if (wo.n) wide_reserve(p, &R.wcand, &R.wcand_cap, wo.n, wo.cw, 0);
+        }
+        for (WideOut& wo : outs) {
+            Relation& R = p->rels[wo.rel];
             for (size_t k = 0; k < wo.rules.size(); k++) {
                 const int q = wo.rules[k];
                 const Rule& ru = s.rules[q];
                 WideRuleRun& r = rr[q];
                 if (!r.active || !r.total) continue;
-                u64* dst = R.wcand + wo.seg_start[k] * (u64)wo.cw;
+                WideExpandJob& j = eb.job[eb.n++];
+                j = WideExpandJob{};
+                j.outer = r.outer;
+                j.inner = r.inner;
+                j.dst = R.wcand + wo.seg_start[k] * (u64)wo.cw;
+                j.no = r.no;
+                j.first = eb.total;
+                j.n = r.pj.n;
+                for (int c = 0; c < r.pj.n; c++) j.src[c] = (unsigned char)r.pj.src[c];
                 if (ru.kind == kJoin) {
-                    wide_join_expand_kernel<<<wide_grid(r.total), kThreads, 0, p->stream>>>(
-                        r.outer, r.inner, r.no, lo + r.off, off + r.off, r.total, r.pj, dst);
+                    j.kind = 0;
+                    j.lo = lo + r.off;
+                    j.off = off + r.off;
+                    j.left = r.pj.left;
+                    j.W0 = r.pj.W0;
+                    j.W1 = r.pj.W1;
+                    j.jcc = r.pj.jcc;
                     p->stats.join_candidates += r.total;
                 } else {
-                    const int Wi = (int)p->rels[ru.in0].arity + 1;
-                    const bool f = ru.kind == RA_COPY_FILTER;
-                    wide_copy_kernel<<<wide_grid(r.no), kThreads, 0, p->stream>>>(r.outer, Wi, r.no, r.pj,
-                                                                                 f ? keep + r.off : nullptr,
-                                                                                 f ? pos + r.off : nullptr, dst);
+                    j.kind = 1;
+                    j.Wi = (int)p->rels[ru.in0].arity + 1;
+                    j.off = ru.kind == RA_COPY_FILTER ? pos + r.off : nullptr;
                 }
-                LAUNCHED();
+                eb.total += r.total;
+                if (eb.n == kWideJobs) flush_expand();
             }
         }
+        flush_expand();
     }
     // 3. winners of every output relation, one round trip for all of them
     u64* picks = tot + nr;   // per relation: kWideMaxSegs + 1 picked counts, then its winner total
     bool any = false;
     {
         PhaseTimer pt(p, 3);
+        WideWinBatch wb{};
+        int wseg = 0;
+        auto flush_win = [&]() {
+            if (!wb.n) return;
+            wide_winners_batch_kernel<<<wb.n, kThreads, 0, p->stream>>>(wb);
+            LAUNCHED();
+            wb.n = 0;
+            wseg = 0;
+        };
         for (size_t k = 0; k < outs.size(); k++) {
             WideOut& wo = outs[k];
             Relation& R = p->rels[wo.rel];
             if (!wo.n) continue;
             any = true;
             const int W = (int)R.arity + 1;
-            const u64* idx = wide_sort(p, R.wcand, wo.cw, wo.cw, wo.n);
             wide_reserve32(p, &R.wflag, &R.wflag_cap, wo.n);
             wide_reserve(p, &R.wpos, &R.wpos_cap, wo.n, 1, 0);
+            u64* my = picks + k * (kWideMaxSegs + 2);
+            const int nseg = (int)wo.rules.size();
+            if (wo.n <= kWideBlockSort) {
+                if (wseg + nseg > 2 * kWideJobs) flush_win();
+                WideWinJob& j = wb.job[wb.n++];
+                j = WideWinJob{R.wcand, R.wfull, R.wdelta, R.wflag, R.wpos, my, wo.n, R.full_n, R.delta_n,
+                               wo.cw, W, wseg, nseg};
+                for (int q = 0; q < nseg; q++) wb.seg_start[wseg + q] = wo.seg_start[q];
+                wseg += nseg;
+                if (wb.n == kWideJobs) flush_win();
+                continue;
+            }
+            const u64* idx = wide_sort(p, R.wcand, wo.cw, wo.cw, wo.n);
             wide_winner_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, idx, wo.n, R.wfull,
                                                                             R.full_n, R.wdelta, R.delta_n, W, R.wflag);
             LAUNCHED();
-            u64* my = picks + k * (kWideMaxSegs + 2);
             wide_scan_async<u32>(p, R.wflag, wo.n, R.wpos, my + kWideMaxSegs + 1);
             WideSegs sg{};
-            sg.n = (int)wo.rules.size();
+            sg.n = nseg;
             for (int j = 0; j < sg.n; j++) sg.start[j] = wo.seg_start[j];
             sg.start[sg.n] = wo.n;
             wide_pick_kernel<<<1, kWideMaxSegs + 1, 0, p->stream>>>(R.wpos, wo.n, my + kWideMaxSegs + 1, sg, my);
             LAUNCHED();
         }
+        flush_win();
         std::vector<u64> h(outs.size() * (kWideMaxSegs + 2));
         if (any) {
             CK(cudaMemcpyAsync(h.data(), picks, h.size() * 8, cudaMemcpyDeviceToHost, p->stream));
@@ -445,42 +505,101 @@ void wide_iteration(ra_program* p, Scc& s)
     // 5. newt rows, sorted into trie order
     {
         PhaseTimer pt(p, 4);
+        u64 small_rows = 0;   // scratch for the batched relations' unsorted rows
+        for (WideOut& wo : outs)
+            if (wo.winners && wo.winners <= kWideBlockSort) small_rows += wo.winners * (p->rels[wo.rel].arity + 1);
+        u64* srows = small_rows ? wide_scratch(p, kWsRows, small_rows) : nullptr;
+        u64 srow_at = 0;
+        WideNewtBatch nb{};
+        int nseg_at = 0;
+        auto flush_newt = [&]() {
+            if (!nb.n) return;
+            wide_newt_batch_kernel<<<nb.n, kThreads, 0, p->stream>>>(nb);
+            LAUNCHED();
+            nb.n = 0;
+            nseg_at = 0;
+        };
         for (WideOut& wo : outs) {
             Relation& R = p->rels[wo.rel];
             if (!wo.winners) continue;
             const int W = (int)R.arity + 1;
+            const int nseg = (int)wo.rules.size();
+            p->stats.new_tuples += wo.winners;
+            if (wo.winners <= kWideBlockSort) {
+                if (nseg_at + nseg > 2 * kWideJobs) flush_newt();
+                WideNewtJob& j = nb.job[nb.n++];
+                j = WideNewtJob{R.wcand, R.wflag, R.wpos, srows + srow_at, R.wnewt, wo.n, wo.winners, wo.cw, W,
+                                nseg_at, nseg};
+                for (int k = 0; k < nseg; k++) {
+                    nb.seg_start[nseg_at + k] = wo.seg_start[k];
+                    nb.win_base[nseg_at + k] = wo.seg_wins[k];
+                    nb.id_base[nseg_at + k] = id_base[wo.rules[k]];
+                }
+                nseg_at += nseg;
+                srow_at += wo.winners * (u64)W;
+                if (nb.n == kWideJobs) flush_newt();
+                continue;
+            }
+            flush_newt();   // the large path reuses the row scratch
+            srow_at = 0;
             WideSegs sg{};
-            sg.n = (int)wo.rules.size();
+            sg.n = nseg;
             for (int k = 0; k < sg.n; k++) {
                 sg.start[k] = wo.seg_start[k];
                 sg.win_base[k] = wo.seg_wins[k];
                 sg.id_base[k] = id_base[wo.rules[k]];
             }
             sg.start[sg.n] = wo.n;
-            u64* rows = wide_scratch(p, kWsRows, wo.winners * (u64)W);
+            u64* rows = wide_scratch(p, kWsRows, std::max<u64>(wo.winners * (u64)W, small_rows));
+            srows = rows;
             wide_newt_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, wo.n, R.wflag, R.wpos, sg,
                                                                            W, rows);
             LAUNCHED();
-            if (wo.winners == 1) {
-                CK(cudaMemcpyAsync(R.wnewt, rows, (u64)W * 8, cudaMemcpyDeviceToDevice, p->stream));
-            } else {
-                const u64* idx = wide_sort(p, rows, W, W, wo.winners);
-                wide_gather_kernel<<<wide_grid(wo.winners * W), kThreads, 0, p->stream>>>(rows, W, idx, wo.winners,
-                                                                                         R.wnewt);
-                LAUNCHED();
-            }
-            p->stats.new_tuples += wo.winners;
+            const u64* idx = wide_sort(p, rows, W, W, wo.winners);
+            wide_gather_kernel<<<wide_grid(wo.winners * W), kThreads, 0, p->stream>>>(rows, W, idx, wo.winners,
+                                                                                     R.wnewt);
+            LAUNCHED();
         }
+        flush_newt();
     }
-    // local_insert_in_full: full = full + delta, delta = newt
-    PhaseTimer pt(p, 5);
-    for (int ri : s.rels) {
-        Relation& R = p->rels[ri];
-        wide_delta_to_full(p, R);
-        std::swap(R.wdelta, R.wnewt);
-        std::swap(R.wdelta_cap, R.wnewt_cap);
-        R.delta_n = R.newt_n;
-        R.newt_n = 0;
+    // local_insert_in_full: full = full + delta (one flattened launch), delta = newt
+    {
+        PhaseTimer pt(p, 5);
+        WideMergeBatch mb{};
+        std::vector<int> merged;
+        auto flush_merge = [&]() {
+            if (!mb.n) return;
+            wide_merge_batch_kernel<<<wide_grid(mb.total), kThreads, 0, p->stream>>>(mb);
+            LAUNCHED();
+            for (int ri : merged) {
+                Relation& R = p->rels[ri];
+                std::swap(R.wfull, R.wspare);
+                std::swap(R.wfull_cap, R.wspare_cap);
+                R.full_n += R.delta_n;
+                R.delta_n = 0;
+            }
+            merged.clear();
+            mb.n = 0;
+            mb.total = 0;
+        };
+        for (int ri : s.rels) {
+            Relation& R = p->rels[ri];
+            if (!R.delta_n) continue;
+            const int W = (int)R.arity + 1;
+            wide_reserve(p, &R.wspare, &R.wspare_cap, R.full_n + R.delta_n, W, 0);
+            mb.job[mb.n++] = WideMergeJob{R.wfull, R.wdelta, R.wspare, R.full_n, R.delta_n, mb.total, W};
+            mb.total += R.full_n + R.delta_n;
+            merged.push_back(ri);
+            if (mb.n == kWideJobs) flush_merge();
+        }
+        flush_merge();
+        for (int ri : s.rels) {
+            Relation& R = p->rels[ri];
+            std::swap(R.wdelta, R.wnewt);
+            std::swap(R.wdelta_cap, R.wnewt_cap);
+            R.delta_n = R.newt_n;
+            R.newt_n = 0;
+        }
     }
     p->stats.iterations++;
 }

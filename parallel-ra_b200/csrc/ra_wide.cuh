@@ -354,6 +354,300 @@ __global__ void wide_pick_kernel(const u64* __restrict__ scanned, u64 n, const u
     if (q <= sg.n) out[q] = sg.start[q] < n ? scanned[sg.start[q]] : *total;
 }
 
+// ---------------------------------------------------------------------------
+// Batched launches: one kernel per phase of an iteration for all of its small
+// rules or relations (one block each, or one flattened index space), with the
+// work list passed as a kernel parameter (no host-to-device copy).  Most
+// iterations of a generated analysis move a few hundred tuples, so launches,
+// not bytes, set their cost.
+// ---------------------------------------------------------------------------
+constexpr int kWideJobs = 64;          // work items per batched launch
+constexpr u32 kWideBlockSort = 1024;   // rows a block sorts in shared memory
+constexpr u32 kWideBlockScan = kThreads * kWideScanPer;   // rows a block counts and scans
+
+// Bitonic sort of s[0..P) (P a power of two; padding holds the sentinel ~0) by
+// (first ncmp columns of rows[s[i]], s[i]), by one block.
+__device__ __forceinline__ void wide_block_sort(u64* s, u32 P, const u64* __restrict__ rows, int W, int ncmp)
+{
+    for (u32 k = 2; k <= P; k <<= 1) {
+        for (u32 j = k >> 1; j > 0; j >>= 1) {
+            for (u32 t = threadIdx.x; t < P; t += blockDim.x) {
+                const u32 partner = t ^ j;
+                if (partner <= t) continue;
+                const u64 a = s[t], b = s[partner];
+                bool a_after_b;
+                if (a == ~0ull) a_after_b = b != ~0ull;
+                else if (b == ~0ull) a_after_b = false;
+                else a_after_b = wide_before(rows, W, ncmp, b, a);
+                if (a_after_b == ((t & k) == 0)) {
+                    s[t] = b;
+                    s[partner] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ u32 wide_pow2(u64 n)
+{
+    u32 P = 2;
+    while (P < n) P <<= 1;
+    return P;
+}
+
+// Phase 1: per job, a join's range counts and their exclusive scan, or a
+// copy_filter's pass flags and their scan; the total into *total.
+struct WideCountJob {
+    const u64* outer;
+    const u64* inner;
+    u64 no, ni;
+    u64* lo;       // join: first match per outer row
+    u64* cnt;      // join: matches per outer row
+    u64* off;      // join: scanned counts; filter: scanned flags
+    u32* keep;     // filter: pass flags
+    u64* total;
+    int Wo, Wi, jcc, pred;   // pred < 0: a join
+};
+struct WideCountBatch {
+    int n;
+    WideCountJob job[kWideJobs];
+};
+
+__global__ void __launch_bounds__(kThreads) wide_count_batch_kernel(const __grid_constant__ WideCountBatch b)
+{
+    __shared__ u64 sm[kWarps + 1];
+    const WideCountJob& j = b.job[blockIdx.x];
+    const u64 base = (u64)threadIdx.x * kWideScanPer;
+    u64 loc = 0;
+    for (int k = 0; k < kWideScanPer; k++) {
+        const u64 o = base + k;
+        if (o >= j.no) break;
+        const u64* row = j.outer + o * (u64)j.Wo;
+        if (j.pred < 0) {
+            const u64 a = j.jcc ? wide_lower_bound(j.inner, j.Wi, j.ni, row, j.jcc) : 0;
+            const u64 e = j.jcc ? wide_upper_bound(j.inner, j.Wi, j.ni, row, j.jcc) : j.ni;
+            j.lo[o] = a;
+            j.cnt[o] = e - a;
+            loc += e - a;
+        } else {
+            const u32 f = eval_pred(j.pred, row[0], j.Wo > 1 ? row[1] : 0) ? 1u : 0u;
+            j.keep[o] = f;
+            loc += f;
+        }
+    }
+    u64 agg;
+    u64 ex = block_exclusive_scan(loc, sm, &agg);
+    for (int k = 0; k < kWideScanPer; k++) {
+        const u64 o = base + k;
+        if (o >= j.no) break;
+        j.off[o] = ex;
+        ex += j.pred < 0 ? j.cnt[o] : (u64)j.keep[o];
+    }
+    if (threadIdx.x == 0) *j.total = agg;
+}
+
+// Phase 2: every rule's candidates in one flattened index space.
+struct WideExpandJob {
+    const u64* outer;   // join: outer rows; copy: input rows
+    const u64* inner;
+    const u64* lo;
+    const u64* off;     // join: scanned counts; filter: scanned pass flags (null for a plain copy)
+    u64* dst;
+    u64 no;
+    u64 first;          // first flattened index of this job
+    int Wi;             // copy: input width
+    int n, left, W0, W1, jcc, kind;   // kind 0: join, 1: copy
+    unsigned char src[kWideMaxCols];
+};
+struct WideExpandBatch {
+    int n;
+    u64 total;
+    WideExpandJob job[kWideJobs];
+};
+
+__global__ void __launch_bounds__(kThreads) wide_expand_batch_kernel(const __grid_constant__ WideExpandBatch b)
+{
+    for (u64 g = (u64)blockIdx.x * kThreads + threadIdx.x; g < b.total; g += (u64)gridDim.x * kThreads) {
+        int r = 0, hi = b.n;   // last job whose first index is <= g
+        while (hi - r > 1) {
+            const int m = (r + hi) >> 1;
+            if (b.job[m].first <= g) r = m;
+            else hi = m;
+        }
+        const WideExpandJob& j = b.job[r];
+        const u64 c = g - j.first;
+        u64* dst = j.dst + c * (u64)j.n;
+        if (j.kind == 0) {
+            u64 a = 0, e = j.no;
+            while (a < e) {
+                const u64 m = (a + e) >> 1;
+                if (j.off[m] <= c) a = m + 1;
+                else e = m;
+            }
+            const u64 o = a - 1, u = j.lo[o] + (c - j.off[o]);
+            const int Wo = j.left ? j.W0 : j.W1, Wi = j.left ? j.W1 : j.W0;
+            const u64* ro = j.outer + o * (u64)Wo;
+            const u64* ri = j.inner + u * (u64)Wi;
+            const u64* r0 = j.left ? ro : ri;
+            const u64* r1 = j.left ? ri : ro;
+            for (int k = 0; k < j.n; k++) {
+                const int x = j.src[k];
+                dst[k] = x < j.W0 ? r0[x] : r1[j.jcc + (x - j.W0)];
+            }
+        } else {
+            u64 rin = c;
+            if (j.off) {   // the c-th kept row: the last row whose scanned flag is <= c
+                u64 a = 0, e = j.no;
+                while (a < e) {
+                    const u64 m = (a + e) >> 1;
+                    if (j.off[m] <= c) a = m + 1;
+                    else e = m;
+                }
+                rin = a - 1;
+            }
+            const u64* row = j.outer + rin * (u64)j.Wi;
+            for (int k = 0; k < j.n; k++) dst[k] = row[j.src[k]];
+        }
+    }
+}
+
+// Phase 3: per relation of at most kWideBlockSort candidates, one block sorts
+// them, flags the winners, scans the flags and picks each rule segment's
+// winners-before count (and the total after the last).
+struct WideWinJob {
+    const u64* cand;
+    const u64* full;
+    const u64* delta;
+    u32* flag;
+    u64* pos;
+    u64* picks;      // seg + 1 values, then the total at picks[kWideMaxSegs + 1]
+    u64 n, nf, nd;
+    int cw, W, seg0, nseg;
+};
+struct WideWinBatch {
+    int n;
+    WideWinJob job[kWideJobs];
+    u64 seg_start[2 * kWideJobs];   // per job: nseg segment starts from seg0
+};
+
+__global__ void __launch_bounds__(kThreads) wide_winners_batch_kernel(const __grid_constant__ WideWinBatch b)
+{
+    __shared__ u64 s[kWideBlockSort];
+    __shared__ u64 sm[kWarps + 1];
+    __shared__ u8 win[kWideBlockSort];
+    const WideWinJob& j = b.job[blockIdx.x];
+    const u32 P = wide_pow2(j.n);
+    for (u32 t = threadIdx.x; t < P; t += blockDim.x) s[t] = t < j.n ? t : ~0ull;
+    __syncthreads();
+    wide_block_sort(s, P, j.cand, j.cw, j.cw);
+    for (u32 k = threadIdx.x; k < j.n; k += blockDim.x) {
+        const u64 c = s[k];
+        const u64* row = j.cand + c * (u64)j.cw;
+        bool w = k == 0 || wide_cmp(j.cand + s[k - 1] * (u64)j.cw, row, j.cw) != 0;
+        if (w) w = !wide_has_prefix(j.full, j.W, j.nf, row, j.cw) && !wide_has_prefix(j.delta, j.W, j.nd, row, j.cw);
+        win[c] = w ? 1 : 0;
+        j.flag[c] = w ? 1u : 0u;
+    }
+    __syncthreads();
+    const u32 per = (u32)((j.n + blockDim.x - 1) / blockDim.x), c0 = threadIdx.x * per;
+    u64 loc = 0;
+    for (u32 k = 0; k < per && c0 + k < j.n; k++) loc += win[c0 + k];
+    u64 agg;
+    u64 ex = block_exclusive_scan(loc, sm, &agg);
+    for (u32 k = 0; k < per && c0 + k < j.n; k++) {
+        s[c0 + k] = ex;   // the sorted order is no longer needed
+        j.pos[c0 + k] = ex;
+        ex += win[c0 + k];
+    }
+    __syncthreads();
+    if ((int)threadIdx.x <= j.nseg) {
+        const u64 st = threadIdx.x < (u32)j.nseg ? b.seg_start[j.seg0 + threadIdx.x] : j.n;
+        j.picks[threadIdx.x] = st < j.n ? s[st] : agg;
+    }
+    if (threadIdx.x == 0) j.picks[kWideMaxSegs + 1] = agg;
+}
+
+// Phase 5: per relation of at most kWideBlockSort new tuples, one block writes
+// the newt rows (ids per rule segment) into `rows`, sorts them into trie order
+// and gathers them into the relation's newt.
+struct WideNewtJob {
+    const u64* cand;
+    const u32* flag;
+    const u64* pos;
+    u64* rows;       // scratch: winners x W
+    u64* newt;
+    u64 n, winners;
+    int cw, W, seg0, nseg;
+};
+struct WideNewtBatch {
+    int n;
+    WideNewtJob job[kWideJobs];
+    u64 seg_start[2 * kWideJobs];
+    u64 win_base[2 * kWideJobs];
+    u64 id_base[2 * kWideJobs];
+};
+
+__global__ void __launch_bounds__(kThreads) wide_newt_batch_kernel(const __grid_constant__ WideNewtBatch b)
+{
+    __shared__ u64 s[kWideBlockSort];
+    const WideNewtJob& j = b.job[blockIdx.x];
+    for (u64 c = threadIdx.x; c < j.n; c += blockDim.x) {
+        if (!j.flag[c]) continue;
+        int q = 0;
+        while (q + 1 < j.nseg && c >= b.seg_start[j.seg0 + q + 1]) q++;
+        const u64 at = j.pos[c];
+        const u64* src = j.cand + c * (u64)j.cw;
+        u64* dst = j.rows + at * (u64)j.W;
+        for (int k = 0; k < j.cw; k++) dst[k] = src[k];
+        if (j.cw < j.W) dst[j.W - 1] = b.id_base[j.seg0 + q] + (at - b.win_base[j.seg0 + q]);
+    }
+    __syncthreads();
+    const u32 P = wide_pow2(j.winners);
+    for (u32 t = threadIdx.x; t < P; t += blockDim.x) s[t] = t < j.winners ? t : ~0ull;
+    __syncthreads();
+    wide_block_sort(s, P, j.rows, j.W, j.W);
+    const u64 total = j.winners * (u64)j.W;
+    for (u64 e = threadIdx.x; e < total; e += blockDim.x) {
+        const u64 k = e / (u64)j.W, c = e - k * (u64)j.W;
+        j.newt[e] = j.rows[s[k] * (u64)j.W + c];
+    }
+}
+
+// Phase 6: full + delta of every relation of the SCC, one flattened index space.
+struct WideMergeJob {
+    const u64* full;
+    const u64* delta;
+    u64* out;
+    u64 nf, nd, first;
+    int W;
+};
+struct WideMergeBatch {
+    int n;
+    u64 total;
+    WideMergeJob job[kWideJobs];
+};
+
+__global__ void __launch_bounds__(kThreads) wide_merge_batch_kernel(const __grid_constant__ WideMergeBatch b)
+{
+    for (u64 g = (u64)blockIdx.x * kThreads + threadIdx.x; g < b.total; g += (u64)gridDim.x * kThreads) {
+        int r = 0, hi = b.n;
+        while (hi - r > 1) {
+            const int m = (r + hi) >> 1;
+            if (b.job[m].first <= g) r = m;
+            else hi = m;
+        }
+        const WideMergeJob& j = b.job[r];
+        const u64 p = g - j.first;
+        const bool fromA = p < j.nf;
+        const u64 i = fromA ? p : p - j.nf;
+        const u64* row = fromA ? j.full + i * (u64)j.W : j.delta + i * (u64)j.W;
+        const u64 rk = fromA ? wide_lower_bound(j.delta, j.W, j.nd, row, j.W) : wide_upper_bound(j.full, j.W, j.nf, row, j.W);
+        u64* dst = j.out + (i + rk) * (u64)j.W;
+        for (int k = 0; k < j.W; k++) dst[k] = row[k];
+    }
+}
+
 // Count and digest of a relation's rows, data columns only (no instances).
 __global__ void __launch_bounds__(kThreads) wide_summary_kernel(const u64* __restrict__ rows, int W, u64 n,
                                                                 u64* __restrict__ acc)
