@@ -430,39 +430,73 @@ void wide_iteration(ra_program* p, Scc& s)
     bool any = false;
     {
         PhaseTimer pt(p, 3);
-        WideWinBatch wb{};
-        int wseg = 0;
-        auto flush_win = [&]() {
-            if (!wb.n) return;
-            wide_winners_batch_kernel<<<wb.n, kThreads, 0, p->stream>>>(wb);
+        // heads: the first of each group of equal candidates
+        WideHeadBatch hb{};
+        auto flush_heads = [&]() {
+            if (!hb.n) return;
+            wide_heads_batch_kernel<<<hb.n, kThreads, 0, p->stream>>>(hb);
             LAUNCHED();
-            wb.n = 0;
-            wseg = 0;
+            hb.n = 0;
         };
         for (size_t k = 0; k < outs.size(); k++) {
             WideOut& wo = outs[k];
             Relation& R = p->rels[wo.rel];
             if (!wo.n) continue;
             any = true;
-            const int W = (int)R.arity + 1;
             wide_reserve32(p, &R.wflag, &R.wflag_cap, wo.n);
             wide_reserve(p, &R.wpos, &R.wpos_cap, wo.n, 1, 0);
-            u64* my = picks + k * (kWideMaxSegs + 2);
-            const int nseg = (int)wo.rules.size();
             if (wo.n <= kWideBlockSort) {
-                if (wseg + nseg > 2 * kWideJobs) flush_win();
-                WideWinJob& j = wb.job[wb.n++];
-                j = WideWinJob{R.wcand, R.wfull, R.wdelta, R.wflag, R.wpos, my, wo.n, R.full_n, R.delta_n,
-                               wo.cw, W, wseg, nseg};
-                for (int q = 0; q < nseg; q++) wb.seg_start[wseg + q] = wo.seg_start[q];
-                wseg += nseg;
-                if (wb.n == kWideJobs) flush_win();
+                hb.job[hb.n++] = WideHeadJob{R.wcand, R.wflag, wo.n, wo.cw};
+                if (hb.n == kWideJobs) flush_heads();
                 continue;
             }
             const u64* idx = wide_sort(p, R.wcand, wo.cw, wo.cw, wo.n);
-            wide_winner_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, idx, wo.n, R.wfull,
-                                                                            R.full_n, R.wdelta, R.delta_n, W, R.wflag);
+            wide_head_flags_kernel<<<wide_grid(wo.n), kThreads, 0, p->stream>>>(R.wcand, wo.cw, idx, wo.n, R.wflag);
             LAUNCHED();
+        }
+        flush_heads();
+        // membership of the heads in full and delta, one thread per candidate of every relation
+        WideMemberBatch mb{};
+        auto flush_member = [&]() {
+            if (!mb.n) return;
+            wide_member_batch_kernel<<<wide_grid(mb.total), kThreads, 0, p->stream>>>(mb);
+            LAUNCHED();
+            mb.n = 0;
+            mb.total = 0;
+        };
+        for (WideOut& wo : outs) {
+            Relation& R = p->rels[wo.rel];
+            if (!wo.n) continue;
+            mb.job[mb.n++] = WideMemberJob{R.wcand, R.wfull, R.wdelta, R.wflag, wo.n, R.full_n, R.delta_n, mb.total,
+                                           wo.cw, (int)R.arity + 1};
+            mb.total += wo.n;
+            if (mb.n == kWideJobs) flush_member();
+        }
+        flush_member();
+        // positions of the winners and each rule segment's winners-before count
+        WideScanBatch sb{};
+        int sseg = 0;
+        auto flush_scan = [&]() {
+            if (!sb.n) return;
+            wide_scan_pick_batch_kernel<<<sb.n, kThreads, 0, p->stream>>>(sb);
+            LAUNCHED();
+            sb.n = 0;
+            sseg = 0;
+        };
+        for (size_t k = 0; k < outs.size(); k++) {
+            WideOut& wo = outs[k];
+            Relation& R = p->rels[wo.rel];
+            if (!wo.n) continue;
+            u64* my = picks + k * (kWideMaxSegs + 2);
+            const int nseg = (int)wo.rules.size();
+            if (wo.n <= kWideBlockScan) {
+                if (sseg + nseg > 2 * kWideJobs) flush_scan();
+                sb.job[sb.n++] = WideScanJob{R.wflag, R.wpos, my, wo.n, sseg, nseg};
+                for (int q = 0; q < nseg; q++) sb.seg_start[sseg + q] = wo.seg_start[q];
+                sseg += nseg;
+                if (sb.n == kWideJobs) flush_scan();
+                continue;
+            }
             wide_scan_async<u32>(p, R.wflag, wo.n, R.wpos, my + kWideMaxSegs + 1);
             WideSegs sg{};
             sg.n = nseg;
@@ -471,7 +505,7 @@ void wide_iteration(ra_program* p, Scc& s)
             wide_pick_kernel<<<1, kWideMaxSegs + 1, 0, p->stream>>>(R.wpos, wo.n, my + kWideMaxSegs + 1, sg, my);
             LAUNCHED();
         }
-        flush_win();
+        flush_scan();
         std::vector<u64> h(outs.size() * (kWideMaxSegs + 2));
         if (any) {
             CK(cudaMemcpyAsync(h.data(), picks, h.size() * 8, cudaMemcpyDeviceToHost, p->stream));

@@ -36,6 +36,44 @@ __device__ __forceinline__ bool wide_before(const u64* __restrict__ rows, int W,
     return c < 0 || (c == 0 && i < j);
 }
 
+// Bitonic sort of s[0..P) (P a power of two; padding holds the sentinel ~0) by
+// (key[i], key2[i] when given, first ncmp columns of rows[s[i]], s[i]), by one
+// block.  The keys ride along in shared memory, so a comparison reads global
+// memory only when they tie: key (and key2) must be consistent with the row
+// order -- the first (and second) column, or a hash for a grouping sort.
+__device__ __forceinline__ void wide_block_sort(u64* s, u64* key, u64* key2, u32 P, const u64* __restrict__ rows,
+                                                int W, int ncmp)
+{
+    for (u32 k = 2; k <= P; k <<= 1) {
+        for (u32 j = k >> 1; j > 0; j >>= 1) {
+            for (u32 t = threadIdx.x; t < P; t += blockDim.x) {
+                const u32 partner = t ^ j;
+                if (partner <= t) continue;
+                const u64 a = s[t], b = s[partner];
+                const u64 ka = key[t], kb = key[partner];
+                const u64 ka2 = key2 ? key2[t] : 0, kb2 = key2 ? key2[partner] : 0;
+                bool a_after_b;
+                if (a == ~0ull) a_after_b = b != ~0ull;
+                else if (b == ~0ull) a_after_b = false;
+                else if (ka != kb) a_after_b = ka > kb;
+                else if (ka2 != kb2) a_after_b = ka2 > kb2;
+                else a_after_b = wide_before(rows, W, ncmp, b, a);
+                if (a_after_b == ((t & k) == 0)) {
+                    s[t] = b;
+                    s[partner] = a;
+                    key[t] = kb;
+                    key[partner] = ka;
+                    if (key2) {
+                        key2[t] = kb2;
+                        key2[partner] = ka2;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // Tile sort: indices [tile * TILE, ...) of `n` rows, bitonic network in shared
 // memory (missing entries are a sentinel that orders last).  Small inputs take
 // a small tile: the network's depth grows with log^2 of the tile.
@@ -44,30 +82,17 @@ __global__ void __launch_bounds__(kThreads) wide_tile_sort_kernel(const u64* __r
                                                                   u64 n, u64* __restrict__ idx)
 {
     __shared__ u64 s[TILE];
+    __shared__ u64 key[TILE];
+    __shared__ u64 key2[TILE];
     const u64 base = (u64)blockIdx.x * TILE;
     for (int t = threadIdx.x; t < TILE; t += kThreads) {
         const u64 g = base + t;
         s[t] = g < n ? g : ~0ull;
+        key[t] = g < n ? rows[g * (u64)W] : ~0ull;
+        key2[t] = (g < n && ncmp > 1) ? rows[g * (u64)W + 1] : 0;
     }
     __syncthreads();
-    for (int k = 2; k <= TILE; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int t = threadIdx.x; t < TILE; t += kThreads) {
-                const int partner = t ^ j;
-                if (partner <= t) continue;
-                const u64 a = s[t], b = s[partner];
-                bool a_after_b;
-                if (a == ~0ull) a_after_b = b != ~0ull;
-                else if (b == ~0ull) a_after_b = false;
-                else a_after_b = wide_before(rows, W, ncmp, b, a);
-                if (a_after_b == ((t & k) == 0)) {
-                    s[t] = b;
-                    s[partner] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
+    wide_block_sort(s, key, key2, TILE, rows, W, ncmp);
     for (int t = threadIdx.x; t < TILE; t += kThreads) {
         const u64 g = base + t;
         if (g < n) idx[g] = s[t];
@@ -128,17 +153,6 @@ __global__ void __launch_bounds__(kThreads) wide_gather_kernel(const u64* __rest
     for (u64 e = (u64)blockIdx.x * kThreads + threadIdx.x; e < total; e += (u64)gridDim.x * kThreads) {
         const u64 k = e / (u64)W, c = e - k * (u64)W;
         out[e] = rows[idx[k] * (u64)W + c];
-    }
-}
-
-// First row of each group of equal first-`ncmp`-column rows, in sorted order.
-__global__ void __launch_bounds__(kThreads) wide_head_kernel(const u64* __restrict__ rows, int W, int ncmp,
-                                                             const u64* __restrict__ idx, u64 n,
-                                                             u32* __restrict__ head)
-{
-    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
-        const u64* r = rows + idx[k] * (u64)W;
-        head[k] = (k == 0 || wide_cmp(rows + idx[k - 1] * (u64)W, r, ncmp) != 0) ? 1u : 0u;
     }
 }
 
@@ -205,34 +219,6 @@ struct WideProj {
     int src[kWideMaxCols];
 };
 
-// Candidate c: outer row o = last row whose offset is <= c, its (c - off[o])-th match.
-__global__ void __launch_bounds__(kThreads) wide_join_expand_kernel(const u64* __restrict__ outer,
-                                                                    const u64* __restrict__ inner, u64 no,
-                                                                    const u64* __restrict__ lo,
-                                                                    const u64* __restrict__ off, u64 total,
-                                                                    WideProj pj, u64* __restrict__ out)
-{
-    const int Wo = pj.left ? pj.W0 : pj.W1, Wi = pj.left ? pj.W1 : pj.W0;
-    for (u64 c = (u64)blockIdx.x * kThreads + threadIdx.x; c < total; c += (u64)gridDim.x * kThreads) {
-        u64 a = 0, b = no;   // upper_bound over the offsets
-        while (a < b) {
-            const u64 m = (a + b) >> 1;
-            if (off[m] <= c) a = m + 1;
-            else b = m;
-        }
-        const u64 o = a - 1, u = lo[o] + (c - off[o]);
-        const u64* ro = outer + o * (u64)Wo;
-        const u64* ri = inner + u * (u64)Wi;
-        const u64* r0 = pj.left ? ro : ri;
-        const u64* r1 = pj.left ? ri : ro;
-        u64* dst = out + c * (u64)pj.n;
-        for (int j = 0; j < pj.n; j++) {
-            const int x = pj.src[j];
-            dst[j] = x < pj.W0 ? r0[x] : r1[pj.jcc + (x - pj.W0)];
-        }
-    }
-}
-
 // copy_filter's predicate on columns 0 and 1 of each input row.
 __global__ void __launch_bounds__(kThreads) wide_filter_kernel(const u64* __restrict__ in, int Wi, u64 n, int pred,
                                                                u32* __restrict__ keep)
@@ -240,39 +226,6 @@ __global__ void __launch_bounds__(kThreads) wide_filter_kernel(const u64* __rest
     for (u64 r = (u64)blockIdx.x * kThreads + threadIdx.x; r < n; r += (u64)gridDim.x * kThreads) {
         const u64* row = in + r * (u64)Wi;
         keep[r] = eval_pred(pred, row[0], Wi > 1 ? row[1] : 0) ? 1u : 0u;
-    }
-}
-
-// copy / acopy / copy_filter (shmap_relation_exp.cpp:116-265): one candidate per
-// input row in trie order; with `keep`, only kept rows, at their scanned positions.
-__global__ void __launch_bounds__(kThreads) wide_copy_kernel(const u64* __restrict__ in, int Wi, u64 n, WideProj pj,
-                                                             const u32* __restrict__ keep, const u64* __restrict__ pos,
-                                                             u64* __restrict__ out)
-{
-    for (u64 r = (u64)blockIdx.x * kThreads + threadIdx.x; r < n; r += (u64)gridDim.x * kThreads) {
-        if (keep && !keep[r]) continue;
-        const u64* row = in + r * (u64)Wi;
-        u64* dst = out + (keep ? pos[r] : r) * (u64)pj.n;
-        for (int j = 0; j < pj.n; j++) dst[j] = row[pj.src[j]];
-    }
-}
-
-// Winners of one relation's candidates (RAM::local_insert_in_newt,
-// src/RAM/RA_tasks.cpp:824-905): in (data columns, position) order, the first
-// of each group of equal candidates wins unless full or delta holds its data
-// columns; later rules' duplicates of earlier rules' winners lose, as against newt.
-__global__ void __launch_bounds__(kThreads) wide_winner_kernel(const u64* __restrict__ cand, int cw,
-                                                               const u64* __restrict__ idx, u64 n,
-                                                               const u64* __restrict__ full, u64 nf,
-                                                               const u64* __restrict__ delta, u64 nd, int W,
-                                                               u32* __restrict__ win)
-{
-    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
-        const u64 c = idx[k];
-        const u64* row = cand + c * (u64)cw;
-        bool w = k == 0 || wide_cmp(cand + idx[k - 1] * (u64)cw, row, cw) != 0;
-        if (w) w = !wide_has_prefix(full, W, nf, row, cw) && !wide_has_prefix(delta, W, nd, row, cw);
-        win[c] = w ? 1u : 0u;
     }
 }
 
@@ -365,28 +318,12 @@ constexpr int kWideJobs = 64;          // work items per batched launch
 constexpr u32 kWideBlockSort = 1024;   // rows a block sorts in shared memory
 constexpr u32 kWideBlockScan = kThreads * kWideScanPer;   // rows a block counts and scans
 
-// Bitonic sort of s[0..P) (P a power of two; padding holds the sentinel ~0) by
-// (first ncmp columns of rows[s[i]], s[i]), by one block.
-__device__ __forceinline__ void wide_block_sort(u64* s, u32 P, const u64* __restrict__ rows, int W, int ncmp)
+// 64-bit hash of a row's first n columns (grouping key of the winner sorts).
+__device__ __forceinline__ u64 wide_row_hash(const u64* __restrict__ row, int n)
 {
-    for (u32 k = 2; k <= P; k <<= 1) {
-        for (u32 j = k >> 1; j > 0; j >>= 1) {
-            for (u32 t = threadIdx.x; t < P; t += blockDim.x) {
-                const u32 partner = t ^ j;
-                if (partner <= t) continue;
-                const u64 a = s[t], b = s[partner];
-                bool a_after_b;
-                if (a == ~0ull) a_after_b = b != ~0ull;
-                else if (b == ~0ull) a_after_b = false;
-                else a_after_b = wide_before(rows, W, ncmp, b, a);
-                if (a_after_b == ((t & k) == 0)) {
-                    s[t] = b;
-                    s[partner] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
+    u64 h = 0x243f6a8885a308d3ull;
+    for (int c = 0; c < n; c++) h = mix64(h ^ (row[c] + 0x9e3779b97f4a7c15ull * (u64)(c + 1)));
+    return h;
 }
 
 __device__ __forceinline__ u32 wide_pow2(u64 n)
@@ -418,23 +355,26 @@ __global__ void __launch_bounds__(kThreads) wide_count_batch_kernel(const __grid
 {
     __shared__ u64 sm[kWarps + 1];
     const WideCountJob& j = b.job[blockIdx.x];
-    const u64 base = (u64)threadIdx.x * kWideScanPer;
-    u64 loc = 0;
-    for (int k = 0; k < kWideScanPer; k++) {
-        const u64 o = base + k;
-        if (o >= j.no) break;
+    // the searches, one row per thread (their latencies overlap)
+    for (u64 o = threadIdx.x; o < j.no; o += blockDim.x) {
         const u64* row = j.outer + o * (u64)j.Wo;
         if (j.pred < 0) {
             const u64 a = j.jcc ? wide_lower_bound(j.inner, j.Wi, j.ni, row, j.jcc) : 0;
             const u64 e = j.jcc ? wide_upper_bound(j.inner, j.Wi, j.ni, row, j.jcc) : j.ni;
             j.lo[o] = a;
             j.cnt[o] = e - a;
-            loc += e - a;
         } else {
-            const u32 f = eval_pred(j.pred, row[0], j.Wo > 1 ? row[1] : 0) ? 1u : 0u;
-            j.keep[o] = f;
-            loc += f;
+            j.keep[o] = eval_pred(j.pred, row[0], j.Wo > 1 ? row[1] : 0) ? 1u : 0u;
         }
+    }
+    __syncthreads();
+    // the scan, contiguous rows per thread
+    const u64 base = (u64)threadIdx.x * kWideScanPer;
+    u64 loc = 0;
+    for (int k = 0; k < kWideScanPer; k++) {
+        const u64 o = base + k;
+        if (o >= j.no) break;
+        loc += j.pred < 0 ? j.cnt[o] : (u64)j.keep[o];
     }
     u64 agg;
     u64 ex = block_exclusive_scan(loc, sm, &agg);
@@ -512,58 +452,123 @@ __global__ void __launch_bounds__(kThreads) wide_expand_batch_kernel(const __gri
     }
 }
 
-// Phase 3: per relation of at most kWideBlockSort candidates, one block sorts
-// them, flags the winners, scans the flags and picks each rule segment's
-// winners-before count (and the total after the last).
-struct WideWinJob {
+// Phase 3a: per relation of at most kWideBlockSort candidates, one block sorts
+// them by (row hash, row, position) and flags the first candidate of each group
+// of equal ones (the group's first occurrence).
+struct WideHeadJob {
+    const u64* cand;
+    u32* flag;
+    u64 n;
+    int cw;
+};
+struct WideHeadBatch {
+    int n;
+    WideHeadJob job[kWideJobs];
+};
+
+__global__ void __launch_bounds__(kThreads) wide_heads_batch_kernel(const __grid_constant__ WideHeadBatch b)
+{
+    __shared__ u64 s[kWideBlockSort];
+    __shared__ u64 key[kWideBlockSort];
+    const WideHeadJob& j = b.job[blockIdx.x];
+    const u32 P = wide_pow2(j.n);
+    // grouping needs equal candidates adjacent (first occurrence first), not trie
+    // order: rows tie on the hash only when equal, but for a 64-bit hash collision,
+    // which the row comparison then orders
+    for (u32 t = threadIdx.x; t < P; t += blockDim.x) {
+        s[t] = t < j.n ? t : ~0ull;
+        key[t] = t < j.n ? wide_row_hash(j.cand + t * (u64)j.cw, j.cw) : ~0ull;
+    }
+    __syncthreads();
+    wide_block_sort(s, key, nullptr, P, j.cand, j.cw, j.cw);
+    for (u32 k = threadIdx.x; k < j.n; k += blockDim.x) {
+        const u64 c = s[k];
+        const bool h = k == 0 || key[k - 1] != key[k] ||
+                       wide_cmp(j.cand + s[k - 1] * (u64)j.cw, j.cand + c * (u64)j.cw, j.cw) != 0;
+        j.flag[c] = h ? 1u : 0u;
+    }
+}
+
+// Heads of a larger relation, from its index sort (trie order).
+__global__ void __launch_bounds__(kThreads) wide_head_flags_kernel(const u64* __restrict__ cand, int cw,
+                                                                   const u64* __restrict__ idx, u64 n,
+                                                                   u32* __restrict__ flag)
+{
+    for (u64 k = (u64)blockIdx.x * kThreads + threadIdx.x; k < n; k += (u64)gridDim.x * kThreads) {
+        const u64 c = idx[k];
+        flag[c] = (k == 0 || wide_cmp(cand + idx[k - 1] * (u64)cw, cand + c * (u64)cw, cw) != 0) ? 1u : 0u;
+    }
+}
+
+// Phase 3b: a head loses when full or delta holds its data columns (all columns
+// for acopy targets); one thread per candidate of every relation.
+struct WideMemberJob {
     const u64* cand;
     const u64* full;
     const u64* delta;
     u32* flag;
-    u64* pos;
-    u64* picks;      // seg + 1 values, then the total at picks[kWideMaxSegs + 1]
-    u64 n, nf, nd;
-    int cw, W, seg0, nseg;
+    u64 n, nf, nd, first;
+    int cw, W;
 };
-struct WideWinBatch {
+struct WideMemberBatch {
     int n;
-    WideWinJob job[kWideJobs];
-    u64 seg_start[2 * kWideJobs];   // per job: nseg segment starts from seg0
+    u64 total;
+    WideMemberJob job[kWideJobs];
 };
 
-__global__ void __launch_bounds__(kThreads) wide_winners_batch_kernel(const __grid_constant__ WideWinBatch b)
+__global__ void __launch_bounds__(kThreads) wide_member_batch_kernel(const __grid_constant__ WideMemberBatch b)
 {
-    __shared__ u64 s[kWideBlockSort];
-    __shared__ u64 sm[kWarps + 1];
-    __shared__ u8 win[kWideBlockSort];
-    const WideWinJob& j = b.job[blockIdx.x];
-    const u32 P = wide_pow2(j.n);
-    for (u32 t = threadIdx.x; t < P; t += blockDim.x) s[t] = t < j.n ? t : ~0ull;
-    __syncthreads();
-    wide_block_sort(s, P, j.cand, j.cw, j.cw);
-    for (u32 k = threadIdx.x; k < j.n; k += blockDim.x) {
-        const u64 c = s[k];
+    for (u64 g = (u64)blockIdx.x * kThreads + threadIdx.x; g < b.total; g += (u64)gridDim.x * kThreads) {
+        int r = 0, hi = b.n;
+        while (hi - r > 1) {
+            const int m = (r + hi) >> 1;
+            if (b.job[m].first <= g) r = m;
+            else hi = m;
+        }
+        const WideMemberJob& j = b.job[r];
+        const u64 c = g - j.first;
+        if (!j.flag[c]) continue;
         const u64* row = j.cand + c * (u64)j.cw;
-        bool w = k == 0 || wide_cmp(j.cand + s[k - 1] * (u64)j.cw, row, j.cw) != 0;
-        if (w) w = !wide_has_prefix(j.full, j.W, j.nf, row, j.cw) && !wide_has_prefix(j.delta, j.W, j.nd, row, j.cw);
-        win[c] = w ? 1 : 0;
-        j.flag[c] = w ? 1u : 0u;
+        if (wide_has_prefix(j.full, j.W, j.nf, row, j.cw) || wide_has_prefix(j.delta, j.W, j.nd, row, j.cw))
+            j.flag[c] = 0u;
     }
-    __syncthreads();
-    const u32 per = (u32)((j.n + blockDim.x - 1) / blockDim.x), c0 = threadIdx.x * per;
+}
+
+// Phase 3c: per relation of at most kWideBlockScan candidates, one block scans
+// the winner flags into positions and picks each rule segment's winners-before
+// count (and the total at picks[kWideMaxSegs + 1]).
+struct WideScanJob {
+    const u32* flag;
+    u64* pos;
+    u64* picks;
+    u64 n;
+    int seg0, nseg;
+};
+struct WideScanBatch {
+    int n;
+    WideScanJob job[kWideJobs];
+    u64 seg_start[2 * kWideJobs];
+};
+
+__global__ void __launch_bounds__(kThreads) wide_scan_pick_batch_kernel(const __grid_constant__ WideScanBatch b)
+{
+    __shared__ u64 sm[kWarps + 1];
+    const WideScanJob& j = b.job[blockIdx.x];
+    const u64 base = (u64)threadIdx.x * kWideScanPer;
     u64 loc = 0;
-    for (u32 k = 0; k < per && c0 + k < j.n; k++) loc += win[c0 + k];
+    for (int k = 0; k < kWideScanPer; k++)
+        if (base + k < j.n) loc += j.flag[base + k];
     u64 agg;
     u64 ex = block_exclusive_scan(loc, sm, &agg);
-    for (u32 k = 0; k < per && c0 + k < j.n; k++) {
-        s[c0 + k] = ex;   // the sorted order is no longer needed
-        j.pos[c0 + k] = ex;
-        ex += win[c0 + k];
-    }
-    __syncthreads();
+    for (int k = 0; k < kWideScanPer; k++)
+        if (base + k < j.n) {
+            j.pos[base + k] = ex;
+            ex += j.flag[base + k];
+        }
+    __syncthreads();   // positions visible to the picking threads
     if ((int)threadIdx.x <= j.nseg) {
         const u64 st = threadIdx.x < (u32)j.nseg ? b.seg_start[j.seg0 + threadIdx.x] : j.n;
-        j.picks[threadIdx.x] = st < j.n ? s[st] : agg;
+        j.picks[threadIdx.x] = st < j.n ? j.pos[st] : agg;
     }
     if (threadIdx.x == 0) j.picks[kWideMaxSegs + 1] = agg;
 }
@@ -591,6 +596,8 @@ struct WideNewtBatch {
 __global__ void __launch_bounds__(kThreads) wide_newt_batch_kernel(const __grid_constant__ WideNewtBatch b)
 {
     __shared__ u64 s[kWideBlockSort];
+    __shared__ u64 key[kWideBlockSort];
+    __shared__ u64 key2[kWideBlockSort];
     const WideNewtJob& j = b.job[blockIdx.x];
     for (u64 c = threadIdx.x; c < j.n; c += blockDim.x) {
         if (!j.flag[c]) continue;
@@ -604,9 +611,13 @@ __global__ void __launch_bounds__(kThreads) wide_newt_batch_kernel(const __grid_
     }
     __syncthreads();
     const u32 P = wide_pow2(j.winners);
-    for (u32 t = threadIdx.x; t < P; t += blockDim.x) s[t] = t < j.winners ? t : ~0ull;
+    for (u32 t = threadIdx.x; t < P; t += blockDim.x) {
+        s[t] = t < j.winners ? t : ~0ull;
+        key[t] = t < j.winners ? j.rows[t * (u64)j.W] : ~0ull;
+        key2[t] = t < j.winners ? j.rows[t * (u64)j.W + 1] : 0;
+    }
     __syncthreads();
-    wide_block_sort(s, P, j.rows, j.W, j.W);
+    wide_block_sort(s, key, key2, P, j.rows, j.W, j.W);
     const u64 total = j.winners * (u64)j.W;
     for (u64 e = threadIdx.x; e < total; e += blockDim.x) {
         const u64 k = e / (u64)j.W, c = e - k * (u64)j.W;
