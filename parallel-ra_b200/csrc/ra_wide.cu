@@ -434,7 +434,7 @@ void wide_iteration(ra_program* p, Scc& s)
         WideHeadBatch hb{};
         auto flush_heads = [&]() {
             if (!hb.n) return;
-            wide_heads_batch_kernel<<<hb.n, kThreads, 0, p->stream>>>(hb);
+            wide_heads_batch_kernel<<<hb.n, kWideWideBlock, 0, p->stream>>>(hb);
             LAUNCHED();
             hb.n = 0;
         };
@@ -548,7 +548,7 @@ void wide_iteration(ra_program* p, Scc& s)
         int nseg_at = 0;
         auto flush_newt = [&]() {
             if (!nb.n) return;
-            wide_newt_batch_kernel<<<nb.n, kThreads, 0, p->stream>>>(nb);
+            wide_newt_batch_kernel<<<nb.n, kWideWideBlock, 0, p->stream>>>(nb);
             LAUNCHED();
             nb.n = 0;
             nseg_at = 0;

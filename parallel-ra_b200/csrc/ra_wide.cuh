@@ -317,6 +317,7 @@ __global__ void wide_pick_kernel(const u64* __restrict__ scanned, u64 n, const u
 constexpr int kWideJobs = 64;          // work items per batched launch
 constexpr u32 kWideBlockSort = 1024;   // rows a block sorts in shared memory
 constexpr u32 kWideBlockScan = kThreads * kWideScanPer;   // rows a block counts and scans
+constexpr int kWideWideBlock = 1024;   // threads of the per-relation sort kernels (no block scan)
 
 // 64-bit hash of a row's first n columns (grouping key of the winner sorts).
 __device__ __forceinline__ u64 wide_row_hash(const u64* __restrict__ row, int n)
@@ -466,7 +467,7 @@ struct WideHeadBatch {
     WideHeadJob job[kWideJobs];
 };
 
-__global__ void __launch_bounds__(kThreads) wide_heads_batch_kernel(const __grid_constant__ WideHeadBatch b)
+__global__ void __launch_bounds__(kWideWideBlock) wide_heads_batch_kernel(const __grid_constant__ WideHeadBatch b)
 {
     __shared__ u64 s[kWideBlockSort];
     __shared__ u64 key[kWideBlockSort];
@@ -593,7 +594,7 @@ struct WideNewtBatch {
     u64 id_base[2 * kWideJobs];
 };
 
-__global__ void __launch_bounds__(kThreads) wide_newt_batch_kernel(const __grid_constant__ WideNewtBatch b)
+__global__ void __launch_bounds__(kWideWideBlock) wide_newt_batch_kernel(const __grid_constant__ WideNewtBatch b)
 {
     __shared__ u64 s[kWideBlockSort];
     __shared__ u64 key[kWideBlockSort];
