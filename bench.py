@@ -202,6 +202,20 @@ def dense_roofline(d, peak, peak_kind):
                                       "(ncu: sm__throughput ~73%, DRAM idle)"}}
 
 
+def reduce_ranks(total_ms, count, device):
+    """Whole-job figures of N independent replicas: the slowest rank's device time
+    (MAX) and the units all ranks processed (SUM).  One rank: unchanged."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(total_ms), int(count)
+    t = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(count)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(c.item())
+
+
 def metric_of(kind):
     return f"{OUTPUT[kind]} tuples/s" if kind == "sg" else METRIC
 
@@ -299,15 +313,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    tc_all = tc
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-        c = torch.tensor([tc], dtype=torch.float64, device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
-        tc_all = int(c.item())
+    total_ms, tc_all = reduce_ranks(sum(step_ms), tc, f"cuda:{local_rank}")
     value = tc_all * args.steps / (total_ms / 1e3)
     st = prog.stats()
 
@@ -354,7 +360,8 @@ def run_ours(args, rank, world, local_rank):
         e2e_s.append(time.perf_counter() - t0)
         d2h = 8 * (2 + sum(2 + 2 * len(x[1]) for x in h))
         assert f == tc
-    e2e = {"value": tc / statistics.mean(e2e_s), "unit": "tuples/s", "h2d_bytes_per_step": int(rows.nbytes),
+    e2e_ms, e2e_units = reduce_ranks(1e3 * statistics.mean(e2e_s), tc, f"cuda:{local_rank}")
+    e2e = {"value": e2e_units / (e2e_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": int(rows.nbytes),
            "d2h_bytes_per_step": int(d2h)}
 
     peak, peak_kind = load_peaks()
@@ -451,12 +458,8 @@ def run_described_ours(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * facts * args.steps / (total_ms / 1e3)
+    total_ms, facts_all = reduce_ranks(sum(step_ms), facts, f"cuda:{local_rank}")
+    value = facts_all * args.steps / (total_ms / 1e3)
     st = prog.stats()
     # device time per phase of the wide iteration (per-launch events, one extra run)
     prog.set_launch_timing(True)
@@ -481,7 +484,8 @@ def run_described_ours(args, rank, world, local_rank):
         assert got == facts
     h2d = int(sum(r.nbytes for r in host_rows.values()))
     d2h = 8 * (2 * len(rels) + sum(2 + 2 * len(x[1]) for x in hist))
-    e2e = {"value": facts / statistics.mean(e2e_s), "unit": "facts/s", "h2d_bytes_per_step": h2d,
+    e2e_ms, e2e_units = reduce_ranks(1e3 * statistics.mean(e2e_s), facts, f"cuda:{local_rank}")
+    e2e = {"value": e2e_units / (e2e_ms / 1e3), "unit": "facts/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": int(d2h)}
     peak, peak_kind = load_peaks()
     dom = max(phases, key=phases.get)
@@ -593,6 +597,8 @@ def run_batched(args, rank, world, local_rank):
     for _ in range(args.warmup):
         one_pass()
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     step_ms, launches = [], 0
     with ClockSampler(local_rank) as clocks:
         for _ in range(args.steps):
@@ -606,7 +612,11 @@ def run_batched(args, rank, world, local_rank):
             b.record(stream)
             torch.cuda.synchronize()
             step_ms.append(a.elapsed_time(b))
-    value = BATCH_COUNT * args.steps / (sum(step_ms) / 1e3)
+    if world > 1:
+        torch.distributed.barrier()
+    # whole job: every rank's batch (its own instances) over the slowest rank's device time
+    total_ms, done = reduce_ranks(sum(step_ms), BATCH_COUNT * args.steps, dev)
+    value = done / (total_ms / 1e3)
 
     # dominant kernel on the largest wave, with per-launch events
     w, base, t, nrows = staged[0]
@@ -642,6 +652,7 @@ def run_batched(args, rank, world, local_rank):
         hist_rows = sum(it for _, it in runner._scc_blocks())
         d2h += 8 * len(w) * (hist_rows + 2 * len(runner.rels))   # per-instance counts + (count, digest)
     e2e_s = time.perf_counter() - t0
+    e2e_ms, e2e_done = reduce_ranks(1e3 * e2e_s, BATCH_COUNT, dev)
     runner.close()          # release its buffers before the plain runs
 
     # serial: plain one-instance-per-run executions of a random sample, each checked against its wave result
@@ -681,7 +692,7 @@ def run_batched(args, rank, world, local_rank):
                    "batched_e2e_over_serial": (BATCH_COUNT / e2e_s) / serial_ips,
                    "bit_exact_mismatches": mismatches},
         "clocks": clocks.summary(),
-        "e2e": {"value": BATCH_COUNT / e2e_s, "unit": "instances/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": e2e_done / (e2e_ms / 1e3), "unit": "instances/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches), "roofline": roofline, "step_ms": step_ms,
     }
@@ -723,6 +734,8 @@ def run_served(args, rank, world, local_rank):
             k = SERVED_COUNT if rate == max(SERVED_RATES) else min(SERVED_COUNT, int(rate * SERVED_POINT_SECONDS))
             stream = clones(reqs[:k])
             w0 = len(server.waves)
+            if world > 1:
+                torch.distributed.barrier()   # every rank's server starts its stream together
             st = run_stream(server, stream, poisson_arrivals(k, rate, 7))
             waves = server.waves[w0:]
             st["rate"] = rate
@@ -752,12 +765,14 @@ def run_served(args, rank, world, local_rank):
     k1 = 1500
     st_one = run_stream(one, clones(reqs[:k1]), poisson_arrivals(k1, max(SERVED_RATES), 7))
     one.close()
+    # whole job: every rank's top-rate stream over the slowest rank's serving time
+    top_ms, served = reduce_ranks(1e3 * st_top["seconds"], len(stream), f"cuda:{local_rank}")
     if rank != 0:
         return None
     h2d = int(sum(r.rows.nbytes for r in stream))
     line = {
-        "metric": "served instances/s", "value": st_top["instances_per_s"], "unit": "instances/s",
-        "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": 1e3 * st_top["seconds"],
+        "metric": "served instances/s", "value": served / (top_ms / 1e3), "unit": "instances/s",
+        "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": top_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": "served", "requests": SERVED_COUNT, "seed": SERVED_SEED,
                    "mix": "80% TC (ER, n log-uniform [64, 16384], degree U[0.8, 2.0]), 20% SG (random trees, "
@@ -775,7 +790,7 @@ def run_served(args, rank, world, local_rank):
         "bit_exact": {"checked": int(len(sample)), "mismatches": mismatches,
                       "against": "plain single-instance runs of the same requests"},
         "clocks": clocks.summary(),
-        "e2e": {"value": st_top["instances_per_s"], "unit": "instances/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": served / (top_ms / 1e3), "unit": "instances/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(8 * 4 * len(stream))},
         "gpu_launches": int(st_top["gpu_launches"]),
     }
@@ -811,10 +826,11 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.impl == "reference":
         line = run_reference_arm(args, rank, world)
-    elif args.workload == "batched":
-        line = run_batched(args, rank, world, local_rank)
-    elif args.workload == "served":
-        line = run_served(args, rank, world, local_rank)
+    elif args.workload in ("batched", "served"):
+        line = (run_batched if args.workload == "batched" else run_served)(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
     elif args.workload in DESCRIBED:
         line = run_described_ours(args, rank, world, local_rank)
         if world > 1:
