@@ -187,7 +187,7 @@ int ra_program_set_launch_timing(ra_program* p, int on);
  * 30 bits, no intern id copied into a data column) runs on the packed path;
  * any other runs with every relation as rows of arity + 1 u64 in trie order
  * (the wide path, ids numbered as the single-rank reference numbers them), which
- * takes no batched instances, checkpoint dumps or restart (RA_E_UNSUPPORTED). */
+ * takes no batched instances (RA_E_UNSUPPORTED). */
 int ra_relation_create(ra_program* p, uint32_t jcc, uint32_t arity, uint32_t tag,
                        const char* name, int version, int* rel_out);
 /* Initial tuples from host rows (arity+1 u64 each).  Replaces

@@ -1283,25 +1283,10 @@ std::vector<unsigned char> graph_signature(ra_program* p, const DevScc& d)
 // src/relation/balanced_hash_relation.cpp:109-430): with per-rank files the rows
 // file is written when not empty and the size file always ("<bytes/24>\n3");
 // with shared files both only when not empty ("<rows>\n<arity+1>").
-void dump_region(ra_program* p, Relation& r, const u64* keys, const u64* ids, u64 n, const std::string& path)
+// One relation version's rows (arity + 1 u64, trie order) into a dump file and its
+// .size, in the layout of relation::parallel_IO (balanced_hash_relation.cpp:109-430).
+void write_rows_file(ra_program* p, const Relation& r, const std::vector<u64>& host, u64 n, const std::string& path)
 {
-    std::vector<u64> host(n * (r.arity + 1));
-    if (n) {
-        u64 *tk, *tv, *rows;
-        dev_alloc(p, &tk, n);
-        dev_alloc(p, &tv, n);
-        dev_alloc(p, &rows, n * (r.arity + 1));
-        CK(cudaMemcpyAsync(tk, keys, n * 8, cudaMemcpyDeviceToDevice, p->stream));
-        CK(cudaMemcpyAsync(tv, ids, n * 8, cudaMemcpyDeviceToDevice, p->stream));
-        sort_rows(p, r, tk, tv, n, r.keys_unique);
-        rows_unpack<<<grid_for(n), kThreads, 0, p->stream>>>(tk, tv, n, (int)r.arity, p->bits, rows);
-        LAUNCHED();
-        CK(cudaMemcpyAsync(host.data(), rows, host.size() * 8, cudaMemcpyDeviceToHost, p->stream));
-        CK(cudaStreamSynchronize(p->stream));
-        dev_free(p, &tk);
-        dev_free(p, &tv);
-        dev_free(p, &rows);
-    }
     const u64 bytes = host.size() * 8;
     const std::string file = p->cp_separate ? path + "_0" : path;
     if (n) {
@@ -1321,6 +1306,39 @@ void dump_region(ra_program* p, Relation& r, const u64* keys, const u64* ids, u6
     }
 }
 
+void dump_region(ra_program* p, Relation& r, const u64* keys, const u64* ids, u64 n, const std::string& path)
+{
+    std::vector<u64> host(n * (r.arity + 1));
+    if (n) {
+        u64 *tk, *tv, *rows;
+        dev_alloc(p, &tk, n);
+        dev_alloc(p, &tv, n);
+        dev_alloc(p, &rows, n * (r.arity + 1));
+        CK(cudaMemcpyAsync(tk, keys, n * 8, cudaMemcpyDeviceToDevice, p->stream));
+        CK(cudaMemcpyAsync(tv, ids, n * 8, cudaMemcpyDeviceToDevice, p->stream));
+        sort_rows(p, r, tk, tv, n, r.keys_unique);
+        rows_unpack<<<grid_for(n), kThreads, 0, p->stream>>>(tk, tv, n, (int)r.arity, p->bits, rows);
+        LAUNCHED();
+        CK(cudaMemcpyAsync(host.data(), rows, host.size() * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        dev_free(p, &tk);
+        dev_free(p, &tv);
+        dev_free(p, &rows);
+    }
+    write_rows_file(p, r, host, n, path);
+}
+
+// The same from a wide relation version (its rows are already in trie order).
+void dump_wide_region(ra_program* p, Relation& r, const u64* rows, u64 n, const std::string& path)
+{
+    std::vector<u64> host(n * (r.arity + 1));
+    if (n) {
+        CK(cudaMemcpyAsync(host.data(), rows, host.size() * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+    }
+    write_rows_file(p, r, host, n, path);
+}
+
 // LIE::create_checkpoint_dump + write_checkpoint_dump (src/lie/lie.cpp:154-193):
 // directory <output>/checkpoint-<scc>-<loop counter>, the executed SCC ids,
 // every relation's full and delta.  `counts` gives (full, delta) per relation.
@@ -1335,6 +1353,11 @@ void write_checkpoint(ra_program* p, int scc_id, const std::vector<std::pair<u64
     for (size_t i = 0; i < p->rels.size(); i++) {
         Relation& r = p->rels[i];
         const u64 fn = counts[i].first, dn = counts[i].second;
+        if (p->wide) {
+            dump_wide_region(p, r, r.wfull, fn, dir + "/" + r.name + "_full");
+            dump_wide_region(p, r, r.wdelta, dn, dir + "/" + r.name + "_delta");
+            continue;
+        }
         dump_region(p, r, r.keys, r.ids, fn, dir + "/" + r.name + "_full");
         dump_region(p, r, r.keys + fn, r.ids + fn, dn, dir + "/" + r.name + "_delta");
     }
@@ -1358,23 +1381,33 @@ std::vector<std::pair<u64, u64>> host_counts(ra_program* p)
 
 // Restart: a relation's delta from <dir>/<name>_delta (LIE::execute, lie.cpp:300-330),
 // appended after its full version; no file, no delta.
-void load_restart_delta(ra_program* p, Relation& r)
+// The rows of a relation's delta dump (none when the file does not exist).
+bool read_restart_rows(ra_program* p, const Relation& r, std::vector<u64>& host, std::string& path)
 {
-    std::string path = p->rs_dir + "/" + r.name + "_delta";
+    path = p->rs_dir + "/" + r.name + "_delta";
     if (p->rs_separate) path += "_0";
-    if (access(path.c_str(), F_OK) != 0) return;
+    if (access(path.c_str(), F_OK) != 0) return false;
     FILE* f = fopen(path.c_str(), "rb");
     if (!f) fail(p, RA_E_IO, "cannot open %s", path.c_str());
     fseek(f, 0, SEEK_END);
     const long bytes = ftell(f);
     fseek(f, 0, SEEK_SET);
     const u64 w = (r.arity + 1) * 8, n = (u64)bytes / w;
-    std::vector<u64> host(n * (r.arity + 1));
+    host.assign(n * (r.arity + 1), 0);
     if (n && fread(host.data(), 1, n * w, f) != n * w) {
         fclose(f);
         fail(p, RA_E_IO, "short read of %s", path.c_str());
     }
     fclose(f);
+    return true;
+}
+
+void load_restart_delta(ra_program* p, Relation& r)
+{
+    std::vector<u64> host;
+    std::string path;
+    if (!read_restart_rows(p, r, host, path)) return;
+    const u64 w = (r.arity + 1) * 8, n = host.size() / (r.arity + 1);
     for (u64 i = 0; i < n; i++)
         for (u32 c = 0; c < r.arity; c++)
             if (host[i * (r.arity + 1) + c] >> p->bits)
@@ -2272,8 +2305,6 @@ void begin_run(ra_program* p)
     }
     if (p->wide) {
         if (p->n_inst) fail(p, RA_E_UNSUPPORTED, "batched instances of a wide-tuple program");
-        if (p->cp_every || !p->rs_dir.empty())
-            fail(p, RA_E_UNSUPPORTED, "checkpoint dumps or restart of a wide-tuple program");
         for (Relation& r : p->rels) wide_load(p, r);
     }
     p->running = true;

@@ -164,6 +164,25 @@ void wide_full_to_delta(ra_program* p, Relation& r)
     r.full_n = 0;
 }
 
+// Restart (LIE::execute, lie.cpp:300-330): the relation's delta from the dump's
+// <name>_delta rows, after any delta present joined full; no file, no delta.
+void wide_load_restart_delta(ra_program* p, Relation& r)
+{
+    std::vector<u64> host;
+    std::string path;
+    if (!read_restart_rows(p, r, host, path)) return;
+    wide_delta_to_full(p, r);
+    const int W = (int)r.arity + 1;
+    const u64 n = host.size() / (u64)W;
+    if (!n) return;
+    u64* raw;
+    dev_alloc(p, &raw, host.size());
+    CK(cudaMemcpyAsync(raw, host.data(), host.size() * 8, cudaMemcpyHostToDevice, p->stream));
+    r.delta_n = wide_sort_unique(p, raw, W, n, &r.wdelta, &r.wdelta_cap);
+    CK(cudaStreamSynchronize(p->stream));
+    dev_free(p, &raw);
+}
+
 // Loaded rows (arity + 1 columns) into the relation's loaded version, in trie
 // order and distinct on all columns, as populate_full inserts them
 // (balanced_hash_relation.cpp:609-793).
@@ -641,8 +660,12 @@ void wide_iteration(ra_program* p, Scc& s)
 // RAM::execute_in_batches driven by LIE::execute (lie.cpp:355-432) for one SCC.
 void run_scc_wide(ra_program* p, Scc& s)
 {
-    for (size_t i = 0; i < s.rels.size(); i++)
-        if (s.init[i]) wide_full_to_delta(p, p->rels[s.rels[i]]);
+    if (!p->rs_dir.empty()) {
+        for (int ri : s.rels) wide_load_restart_delta(p, p->rels[ri]);
+    } else {
+        for (size_t i = 0; i < s.rels.size(); i++)
+            if (s.init[i]) wide_full_to_delta(p, p->rels[s.rels[i]]);
+    }
     std::vector<uint64_t> hist;
     for (;;) {
         uint32_t b = p->batch_size;
@@ -658,6 +681,7 @@ void run_scc_wide(ra_program* p, Scc& s)
         }
         hist.push_back(d);
         hist.push_back(f);
+        checkpoint_batch(p, s, !s.fixpoint || d == 0, host_counts(p));
         if (!s.fixpoint || d == 0) break;
     }
     CK(cudaStreamSynchronize(p->stream));

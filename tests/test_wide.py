@@ -221,3 +221,71 @@ def test_wide_equals_packed_at_scale():
     assert np.array_equal(a, b)
     w.close()
     k.close()
+
+
+@pytest.mark.gpu
+def test_wide_checkpoint_dumps(tmp_path):
+    """Dumps after every batch of a wide program (the reference's layout: rows of
+    arity + 1 u64 in trie order, per relation <name>_full / <name>_delta + .size) leave
+    the results the reference's, and the last dump holds every relation's rows."""
+    prog = "cfa-4-4-64"
+    p = P.Program(0)
+    p.set_checkpoint(str(tmp_path / "cp"), 1)
+    h = run_described(p, prog)
+    check_against_golden(p, h, load_golden(prog))
+    dumps = os.listdir(tmp_path / "cp")
+    hist = load_golden(prog)["history"]
+    assert len(dumps) == sum(len(b[1]) for b in hist)
+    # the last dump: the last batch of the last SCC (batch numbers restart with each SCC)
+    last_scc = hist[-1][0]
+    last = tmp_path / "cp" / max((d for d in dumps if d.startswith(f"checkpoint-{last_scc}-")),
+                                 key=lambda d: int(d.split("-")[2]))
+    for name, rel in h.items():
+        if name.startswith("__"):
+            continue
+        parts = []
+        for v in ("full", "delta"):
+            f = last / f"{name}_{v}"
+            if f.exists():
+                parts.append(P.datagen.read_relation(str(f)))
+        got = np.concatenate(parts) if parts else np.empty((0, p._arity[rel] + 1), dtype=np.uint64)
+        want = p.dump_full(rel)
+        assert np.array_equal(got[np.lexsort(got.T[::-1])], want), name
+    p.close()
+
+
+@pytest.mark.gpu
+def test_wide_restart_from_own_dump(tmp_path):
+    """TC on values above 2^45 (wide path): dump every 2 batches, restart from a dump in
+    the middle of the fixpoint SCC; the copy SCC is not run again and the closure's
+    tuples equal a straight run's."""
+    rows = P.datagen.with_row_ids(P.datagen.erdos_renyi(400, 600, 9))
+    rows[:, :2] += np.uint64(BIG)
+    p = P.Program(0)
+    rels = P.programs.build_tc(p, rows)
+    p.set_checkpoint(str(tmp_path / "cp"), 2)
+    p.execute(1)
+    want = p.dump_full(rels["T"])[:, :2]
+    mids = sorted((int(d.split("-")[2]), d) for d in os.listdir(tmp_path / "cp") if d.startswith("checkpoint-1-"))
+    dump = str(tmp_path / "cp" / mids[len(mids) // 2][1])
+    assert open(os.path.join(dump, "scc_metadata")).read().split() == ["2"]
+    q = P.Program(0)
+    T = q.relation(1, 2, 257, "T", P.engine.FULL)
+    G = q.relation(1, 2, 256, "G", P.engine.FULL)
+    q.load_file(T, os.path.join(dump, "T_full"))
+    q.load_file(G, os.path.join(dump, "G_full"))
+    join = q.scc(True, 1)
+    q.add_relation(join, G, False)
+    q.add_relation(join, T, True)
+    q.join(join, T, T, P.engine.DELTA, G, P.engine.FULL, [3, 1])
+    copy = q.scc(False, 2)
+    q.add_relation(copy, G, False)
+    q.add_relation(copy, T, True)
+    q.copy(copy, T, G, P.engine.FULL, [1, 0])
+    q.depend(copy, join)
+    q.set_restart(dump)
+    q.execute(1)
+    assert np.array_equal(q.dump_full(T)[:, :2], want)
+    assert [sid for sid, _ in q.history()] == [1]
+    p.close()
+    q.close()
