@@ -119,3 +119,29 @@ def test_large_tc_requests_wave_apart_from_dense_ones():
     s._busy[0] = False
     _, picked, _ = s._take_wave(0)
     assert [r.rid for r in picked] == [1, 3]
+
+
+def test_worker_failure_names_the_wave_and_stops_the_workers():
+    """A wave that fails with an engine error (not out of memory) ends the stream:
+    drain() raises, the failed wave's worker, kind and request ids are recorded, and
+    every worker thread has stopped before the error reaches the caller."""
+    s = Server(slots=2, budget_bytes=1e9, start=False)
+
+    class FailingRunner:
+        prog = None
+
+        def run_wave(self, rows):
+            raise P.RAError(1, "bad argument")
+
+        def close(self):
+            pass
+    s._runners = [{"tc": FailingRunner()}, {"tc": FailingRunner()}]
+    for t in s._workers:
+        t.start()
+    s.submit(fake(7, "tc", 10))
+    with pytest.raises(RuntimeError):
+        s.drain(1, timeout=10)
+    assert len(s.failed_waves) == 1
+    w, kind, rids = s.failed_waves[0]
+    assert kind == "tc" and rids == [7] and w in (0, 1)
+    assert not any(t.is_alive() for t in s._workers)
