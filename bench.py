@@ -235,6 +235,31 @@ def run_reference_arm(args, rank, world):
                 "cpu_baseline": {"value": facts / secs, "unit": "facts/s", "cores": 1, "kind": "reference",
                                  "sample": sample},
                 "e2e": {"value": facts / secs, "unit": "facts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "served":
+        # the reference serves one request at a time: its throughput on a bounded sample of
+        # the served mix (requests whose closure is estimated below 5e6 tuples), converted
+        # to instances/s over the whole mix by the mix's estimated tuples
+        from parallel_ra_b200.batch import estimate_tuples
+        from parallel_ra_b200.serve import request_mix
+        reqs = request_mix(SERVED_COUNT, SERVED_SEED, processes=gen_processes())
+        est = [estimate_tuples(r.kind, r.rows) for r in reqs]
+        rng = np.random.default_rng(7)
+        pool = [int(i) for i in rng.permutation(len(reqs)) if est[int(i)] < 5e6][:BATCH_CPU_SAMPLE]
+        tup = secs = 0.0
+        kind = "port"
+        for i in pool:
+            t, sec, kind = reference_rows_run(reqs[i].rows, reqs[i].kind)
+            tup += t
+            secs += sec
+        value = len(reqs) / (sum(est) / (tup / secs))
+        sample = (f"{len(pool)} random requests of the mix with estimated closure < 5e6 tuples ({int(tup)} "
+                  f"tuples, {secs:.1f} s fixpoint time); instances/s = requests / (mix tuples / sample tuples/s)")
+        return {"impl": "reference", "metric": "served instances/s", "value": value, "unit": "instances/s",
+                "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * len(reqs) / value,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": "served", "requests": SERVED_COUNT, "metric_family": METRIC_FAMILY},
+                "cpu_baseline": {"value": value, "unit": "instances/s", "cores": 1, "kind": kind, "sample": sample},
+                "e2e": {"value": value, "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "batched":
         from parallel_ra_b200.batch import estimate_tuples
         insts = batched_instances(BATCH_COUNT, BATCH_SEED)
