@@ -3,22 +3,29 @@
 // engine's allocation, scan and error helpers.
 //
 // A program runs wide when some relation's tuples do not pack into one 63-bit
-// key, a relation has more than kMaxArity columns or joins on zero columns, or
-// a join key exceeds the CSR index's 30 bits.  Every relation version is then an
+// key, a relation has more than kMaxArity columns or joins on zero columns, a
+// join key exceeds the CSR index's 30 bits, or a rule copies an intern id into a
+// data column.  Every relation version is then an
 // array of arity + 1 u64 rows in trie order, and one iteration of an SCC is
 // RAM::local_compute + local_insert_in_newt + local_insert_in_full
 // (src/RAM/RA_tasks.cpp:305-555, 824-905; balanced_hash_relation.cpp:1120-1231):
 //   1. each rule's candidates, in the reference's emission order (outer rows in
 //      trie order, each one's inner matches in trie order; copies in input order),
 //      written into its output relation's candidate buffer after the earlier rules';
-//   2. per output relation: an index sort of the candidates by (data columns,
-//      position); the first of each group wins unless full or delta holds it;
+//   2. per output relation: an index sort that puts equal candidates next to each
+//      other in position order; the first of each group wins unless full or delta
+//      holds it;
 //   3. ids (tag << 46) | counter assigned to the winners rule by rule in the SCC's
 //      rule order, the counters shared by the relations of one tag, as the
 //      single-rank reference interns them (bucket 0);
 //   4. newt sorted into trie order; full = full + delta (a rank merge), delta = newt.
 // Intern ids therefore equal the reference's, and with them every data column
 // that a rule copies out of an id (acopy).
+//
+// An iteration makes two host round trips (candidate counts; winner counts) and
+// runs each phase for all of its small rules or relations in one batched launch
+// (work lists as kernel parameters), so its cost is a few dozen launches
+// however few tuples it moves.
 //
 // (Included inside the engine's anonymous namespace.)
 

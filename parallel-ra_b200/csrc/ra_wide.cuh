@@ -5,10 +5,12 @@
 // lexicographic over all columns, the order in which the reference's tries
 // enumerate tuples (src/relation/shmap_relation_exp.cpp:77-112).
 //
-// Operations are index sorts with a row comparator (bitonic tiles in shared
-// memory, then merge passes by binary-searched ranks), prefix binary searches
-// (join ranges on the first jcc columns; membership on the data columns), and
-// rank merges of sorted arrays.  All integer, HBM/L2-bound.
+// Operations are index sorts with a row comparator (bitonic networks in shared
+// memory with the first key columns, or a row hash, cached beside each index;
+// merge passes by binary-searched ranks for larger inputs), prefix binary
+// searches (join ranges on the first jcc columns; membership on the data
+// columns), and rank merges of sorted arrays.  All integer; with the small deltas
+// of the generated analyses, latency-bound.
 #pragma once
 
 #include "ra_iter.cuh"
