@@ -87,8 +87,10 @@ typedef struct ra_stats {
     uint64_t dedup_bytes;       /* algorithmic bytes moved by those kernels */
     uint32_t value_bits;        /* bits per packed column chosen for the run */
     uint32_t reserved;
-    /* Device time per phase of the device-driven iterations, filled only when
-     * the program runs with per-launch events (RA_KERNEL_EVENTS=1; no graph):
+    /* Device time per phase of the device-driven iterations: from the
+     * persistent SCC kernel's own clocks (barrier to barrier: [2] claims incl.
+     * heavy rows, [3] select + iteration end), or, for the per-launch kernels,
+     * only with per-launch events (RA_KERNEL_EVENTS=1; no graph):
      * [0] join scan, [1] plan, [2] expand + claim, [3] select, [4] sort,
      * [5] iteration end. */
     double phase_ms[6];
@@ -103,6 +105,8 @@ typedef struct ra_stats {
     double dense_search_ms;
     double dense_emit_ms;
     uint64_t bitmap_relations;  /* output relations of device-driven SCCs that used a bitmap seen set */
+    uint64_t persistent_launches; /* cooperative launches of the persistent SCC kernel (one per SCC run,
+                                     plus one per replay after a buffer grew) */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose

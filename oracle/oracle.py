@@ -59,6 +59,8 @@ def lib():
         L.oracle_dump_full.restype = C.c_uint64
         L.oracle_fixpoint_seconds.argtypes = [P]
         L.oracle_fixpoint_seconds.restype = C.c_double
+        L.oracle_tc_distance_histogram.argtypes = [u64p, u64p, C.c_uint64, C.c_uint64, u64p, C.c_uint64, C.c_int]
+        L.oracle_tc_distance_histogram.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -144,3 +146,22 @@ class OracleProgram:
 
     def fixpoint_seconds(self):
         return float(self._L.oracle_fixpoint_seconds(self._p))
+
+
+def tc_distance_histogram(edges: np.ndarray, n: int, cap: int = 4096, threads: int = 0) -> np.ndarray:
+    """hist[d] = pairs (x, z) of the graph whose shortest path from x to z has d
+    edges (the shortest cycle through x for z == x), over every source x.
+
+    Independent of the reference's algorithm: semi-naive transitive closure adds
+    the pairs at distance k + 2 in its k-th join iteration, so its per-iteration
+    delta sizes must equal hist[2:], and its base (T = G) must hold hist[1] pairs.
+    """
+    src = np.ascontiguousarray(edges[:, 0], dtype=np.uint64)
+    dst = np.ascontiguousarray(edges[:, 1], dtype=np.uint64)
+    hist = np.zeros(cap, dtype=np.uint64)
+    deep = lib().oracle_tc_distance_histogram(_u64(src), _u64(dst), src.size, n, _u64(hist), cap,
+                                              threads or (os.cpu_count() or 1))
+    if deep == 2 ** 64 - 1:
+        raise ValueError("a shortest path is longer than the histogram holds")
+    return hist[:deep + 1]
+

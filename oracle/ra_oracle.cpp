@@ -19,6 +19,8 @@
 #include <set>
 #include <string>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 namespace {
 
@@ -385,5 +387,83 @@ uint64_t oracle_dump_full(oracle_prog* p, int rel, uint64_t* out, uint64_t cap_r
 }
 
 double oracle_fixpoint_seconds(oracle_prog* p) { return p->fixpoint_s; }
+
+// Independent check of transitive closure (not a restatement of the reference):
+// semi-naive TC over the rule T(z, x) :- T_delta(y, x), G(y, z) adds, at
+// iteration k, exactly the pairs (x, z) whose shortest path from x to z has
+// length k + 2 counted in edges (k + 1 for the copy SCC's base T = G), the
+// shortest cycle through x for z == x.  hist[d] += number of pairs at shortest
+// distance d, over every source, by one breadth-first search per source
+// (`threads` threads, sources split in blocks).  Returns the largest distance
+// seen, or ~0 when a distance reaches `cap`.
+uint64_t oracle_tc_distance_histogram(const uint64_t* src, const uint64_t* dst, uint64_t m, uint64_t n,
+                                      uint64_t* hist, uint64_t cap, int threads)
+{
+    std::vector<uint64_t> off(n + 1, 0);
+    for (uint64_t e = 0; e < m; e++) off[src[e] + 1]++;
+    for (uint64_t v = 0; v < n; v++) off[v + 1] += off[v];
+    std::vector<uint32_t> adj(m);
+    {
+        std::vector<uint64_t> cur(off.begin(), off.end() - 1);
+        for (uint64_t e = 0; e < m; e++) adj[cur[src[e]]++] = (uint32_t)dst[e];
+    }
+    if (threads < 1) threads = 1;
+    std::vector<std::vector<uint64_t>> part(threads, std::vector<uint64_t>(cap, 0));
+    std::vector<uint64_t> deepest(threads, 0);
+    std::atomic<uint64_t> next{0};
+    auto work = [&](int t) {
+        std::vector<uint32_t> seen(n, 0);   // stamp of the search that reached the value
+        std::vector<uint32_t> frontier, nxt;
+        uint32_t stamp = 0;
+        for (;;) {
+            const uint64_t s0 = next.fetch_add(4096);
+            if (s0 >= n) break;
+            const uint64_t s1 = std::min<uint64_t>(n, s0 + 4096);
+            for (uint64_t s = s0; s < s1; s++) {
+                ++stamp;
+                frontier.assign(1, (uint32_t)s);
+                bool self = false;
+                for (uint64_t d = 1; !frontier.empty(); d++) {
+                    nxt.clear();
+                    uint64_t found = 0;
+                    for (uint32_t u : frontier)
+                        for (uint64_t e = off[u]; e < off[u + 1]; e++) {
+                            const uint32_t v = adj[e];
+                            if (v == s) {
+                                if (!self) {   // the shortest cycle through s
+                                    self = true;
+                                    found++;
+                                }
+                                continue;
+                            }
+                            if (seen[v] == stamp) continue;
+                            seen[v] = stamp;
+                            nxt.push_back(v);
+                            found++;
+                        }
+                    if (found) {
+                        if (d >= cap) {
+                            deepest[t] = ~0ull;
+                            return;
+                        }
+                        part[t][d] += found;
+                        if (deepest[t] != ~0ull) deepest[t] = std::max(deepest[t], d);
+                    }
+                    frontier.swap(nxt);
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++) pool.emplace_back(work, t);
+    for (auto& th : pool) th.join();
+    uint64_t deep = 0;
+    for (int t = 0; t < threads; t++) {
+        if (deepest[t] == ~0ull) return ~0ull;
+        deep = std::max(deep, deepest[t]);
+        for (uint64_t d = 0; d < cap; d++) hist[d] += part[t][d];
+    }
+    return deep;
+}
 
 }  // extern "C"

@@ -55,6 +55,10 @@ uint64_t oracle_full_count(oracle_prog* p, int rel);
 /* full relation rows (arity+1 u64 each, trie order); returns rows written */
 uint64_t oracle_dump_full(oracle_prog* p, int rel, uint64_t* out, uint64_t cap_rows);
 double oracle_fixpoint_seconds(oracle_prog* p);
+/* Shortest-path-length histogram of a directed graph over every source
+ * (independent check of transitive closure's per-iteration deltas). */
+uint64_t oracle_tc_distance_histogram(const uint64_t* src, const uint64_t* dst, uint64_t m, uint64_t n,
+                                      uint64_t* hist, uint64_t cap, int threads);
 
 #ifdef __cplusplus
 }

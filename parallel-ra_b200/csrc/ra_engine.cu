@@ -17,6 +17,7 @@
 //     device counters.
 #include "../../include/ra_engine.h"
 #include "ra_dense.cuh"
+#include "ra_persist.cuh"
 #include "ra_wide.cuh"
 
 #include <algorithm>
@@ -207,6 +208,8 @@ struct ra_program {
     u64* sort_v[2] = {};
     u64* status = nullptr;
     u64 status_cap = 0;
+    HeavyItem* dheavy = nullptr;  // heavy-row work items of the persistent SCC kernel
+    u64 heavy_cap = 0;
     // instances (batched programs): instance i owns values [inst_base_h[i], inst_base_h[i + 1])
     std::vector<u64> inst_base_h;  // n_inst + 1 entries, the last ~0
     u64* dinst_base = nullptr;
@@ -235,6 +238,7 @@ struct ra_program {
     u64 bmt_rows = 0, bmt_total = 0;
     std::vector<u64> bmt_bases;      // the instance bases the tables were built for
     bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
+    bool use_persist = false;     // RA_PERSIST=1: the persistent SCC kernel instead of CUDA-graph iterations
     bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
 
@@ -1064,11 +1068,20 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     for (int sl = 0; sl < d.plan.n_rels; sl++)
         if (d.bit[sl].seen) bit_rows = std::max<u64>(bit_rows, d.bit[sl].n);
     u64 st_need = std::max<u64>({max_outer / kJRows + 2, p->dcand_cap / kSelTile + 2,
-                                 (p->stage_cap / kSortTile + 2) * kRadix, bit_rows / kWarps + 2});
+                                 (p->stage_cap / kSortTile + 2) * kRadix, bit_rows / kWarps + 2,
+                                 max_outer / kPJChunk + 2, p->dcand_cap / kPSChunk + 2});
     if (st_need > p->status_cap) {
         dev_free(p, &p->status);
         dev_alloc(p, &p->status, st_need);
         p->status_cap = st_need;
+    }
+    // heavy-row slices: at most one per kHeavyPiece candidates plus one per heavy row
+    const u64 heavy_need = p->dcand_cap / kHeavyPiece + p->dcand_cap / kHeavyRow + 64;
+    if (heavy_need > p->heavy_cap) {
+        dev_free(p, &p->dheavy);
+        p->heavy_cap = 0;
+        dev_alloc(p, &p->dheavy, heavy_need);
+        p->heavy_cap = heavy_need;
     }
     if (hist_cap > p->dhist_cap) {
         // layout: hist_cap (sum_delta, sum_full) pairs, then hist_cap iteration end times
@@ -1574,6 +1587,68 @@ void ctl_download(ra_program* p)
     CK(cudaStreamSynchronize(p->stream));
 }
 
+// Kernel parameters of the persistent SCC kernel (ra_persist.cuh) for the plan's
+// current buffers and capacities.
+PersistArgs persist_args(ra_program* p, const DevScc& d)
+{
+    PersistArgs A{};
+    A.ctl = p->ctl;
+    A.plan = d.plan;
+    A.rm = d.rm;
+    A.bits = p->bits;
+    A.cand = p->dcand;
+    A.loser = p->dloser;
+    A.status = p->status;
+    A.status_cap = p->status_cap;
+    A.heavy = p->dheavy;
+    A.heavy_cap = p->heavy_cap;
+    A.history = p->dhist;
+    for (int q = 0; q < d.plan.n_rules; q++) {
+        const DevRule& r = d.rules[q];
+        Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
+        PRule& P = A.rule[q];
+        P.kind = r.kind == kJoin ? kJoinRule : r.kind;
+        P.out_slot = r.out_slot;
+        P.in = r.in;
+        P.pj = r.pj;
+        P.csr = r.csr;
+        P.inner = r.inner;
+        P.outer_shift = r.outer_shift;
+        P.pred = r.pred;
+        P.seen = out.seen;
+        P.seen_cap = out.seen_cap;
+        P.dst_keys = out.keys;
+        P.dst_ids = out.ids;
+        P.inst_shift = (int)(out.arity - 1) * p->bits;
+    }
+    if (p->n_inst) {
+        A.inst_base = p->dinst_base;
+        A.n_inst = p->n_inst;
+        A.inst_new = p->dinst_new;
+        A.inst_iter_cap = p->inst_rows_cap;
+    }
+    return A;
+}
+
+// One cooperative launch of the persistent SCC kernel: every block resident at
+// once (its grid barriers wait on all of them), as many as the device holds.
+void launch_persistent(ra_program* p, const DevScc& d)
+{
+    static int occ = 0, sms = 0;
+    if (!occ) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scc_persistent_kernel, kThreads, 0));
+        if (occ < 1) fail(p, RA_E_CUDA, "the persistent SCC kernel does not fit on an SM");
+    }
+    PersistArgs A = persist_args(p, d);
+    void* args[] = {&A};
+    CK(cudaLaunchCooperativeKernel((const void*)scc_persistent_kernel, dim3(sms * occ), dim3(kThreads), args, 0,
+                                   p->stream));
+    LAUNCHED();
+}
+
 void run_scc_device(ra_program* p, Scc& s, DevScc& d)
 {
     const SccPlan& pl = d.plan;
@@ -1625,10 +1700,21 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     LAUNCHED();
 
     int body_kernels = 0;
-    const bool graph_mode = p->use_graphs && !p->kernel_events && s.fixpoint && !p->cp_every;
+    bool any_bitmap = false;
+    for (int sl = 0; sl < pl.n_rels; sl++) any_bitmap = any_bitmap || d.bit[sl].seen;
+    // the whole fixed point as one cooperative launch: default id order, hash seen sets
+    const bool persist_mode = p->use_persist && p->use_graphs && !p->kernel_events && !p->cp_every &&
+                              p->id_order == RA_IDS_EMISSION && !any_bitmap && pl.n_rules > 0;
+    const bool graph_mode = !persist_mode && p->use_graphs && !p->kernel_events && s.fixpoint && !p->cp_every;
     u64 hist_seen = 0;   // history entries (completed batches) already checkpointed
     for (;;) {
-        if (graph_mode) {
+        if (persist_mode) {
+            h.bar_count = 0;
+            CK(cudaMemcpyAsync(&p->ctl->bar_count, &h.bar_count, 4, cudaMemcpyHostToDevice, p->stream));
+            launch_persistent(p, d);
+            p->stats.persistent_launches++;
+            ctl_download(p);
+        } else if (graph_mode) {
             std::vector<unsigned char> sig = graph_signature(p, d);
             if (s.exec && sig != s.graph_sig) drop_graph(s);
             if (!s.exec) {
@@ -1712,8 +1798,12 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             if (p->n_inst && h.iteration >= p->inst_rows_cap) size_instance_rows(p, 2 * p->inst_rows_cap);
             h.flags = 0;
             h.exit_ctr = 0;
-            if (replay)
+            h.bar_count = 0;
+            if (replay) {
                 for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
+                h.heavy_n = 0;
+                h.heavy_ctr = 0;
+            }
             CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
             if (replay) {
                 CK(cudaMemsetAsync(&p->ctl->sort_hist[0][0][0], 0, sizeof(p->ctl->sort_hist), p->stream));
@@ -1768,6 +1858,10 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
         if (d.bit[sl].seen && r.seen) r.seen_dirty = true;   // its hash set missed this SCC's tuples
     }
     for (size_t t = 0; t < d.tags.size(); t++) intern_counter(p, d.tags[t]) = h.intern[t];
+    if (persist_mode) {   // the persistent kernel's own phase clocks (barrier to barrier)
+        p->stats.phase_ms[2] += (double)(h.ns_claims + h.ns_heavy) / 1e6;
+        p->stats.phase_ms[3] += (double)h.ns_select / 1e6;
+    }
     p->epoch = h.epoch;
     p->stats.iterations += h.iteration;
     p->stats.join_candidates += h.candidates;
@@ -2267,6 +2361,8 @@ void release_buffers(ra_program* p)
     p->stage_cap = 0;
     dev_free(p, &p->status);
     p->status_cap = 0;
+    dev_free(p, &p->dheavy);
+    p->heavy_cap = 0;
     dev_free(p, &p->dinst_new);
     p->inst_rows_cap = 0;
     dev_free(p, &p->dhist);
@@ -2439,6 +2535,7 @@ int ra_program_create(int device, ra_program** out)
         dev_alloc(p, &p->ctl, 1);
         CK(cudaMallocHost(&p->hctl, sizeof(IterCtl)));
         if (const char* e = getenv("RA_NO_GRAPH")) p->use_graphs = atoi(e) == 0;
+        if (const char* e = getenv("RA_PERSIST")) p->use_persist = atoi(e) != 0;
         if (const char* e = getenv("RA_KERNEL_EVENTS")) p->kernel_events = atoi(e) != 0;
     });
     if (st != RA_OK) {
@@ -2490,6 +2587,7 @@ int ra_program_destroy(ra_program* p)
         dev_free(p, &p->sort_v[b]);
     }
     dev_free(p, &p->status);
+    dev_free(p, &p->dheavy);
     dev_free(p, &p->dhist);
     dev_free(p, &p->dinst_base);
     dev_free(p, &p->dinst_new);

@@ -59,6 +59,17 @@ struct IterCtl {
     u32 exit_ctr;                   // blocks of the running select launch that have finished
     u32 flags;
     u32 done;
+    // persistent SCC kernel (ra_persist.cuh): heavy-row work items of the running
+    // iteration, and the grid barrier with the values its last arriver publishes
+    u32 heavy_ctr;                  // items taken
+    u64 heavy_n;                    // items pushed
+    u64 ns_claims, ns_heavy, ns_select;   // device time of the phases of the persistent kernel (ns)
+    u64 t_phase;                    // %globaltimer at the last barrier release (or kernel start)
+    u32 bar_count;                  // blocks arrived at the running barrier
+    u32 bar_gen;                    // barrier generation (bumped on release)
+    u32 bar_flags;                  // flags / done / heavy_n as the last arriver saw them
+    u32 bar_done;
+    u64 bar_heavy;
     u64 sort_hist[kMaxSccRels][kMaxPasses][kRadix];
 };
 
@@ -635,6 +646,8 @@ __device__ void end_of_iteration(IterCtl* __restrict__ ctl, const SccPlan& plan,
         }
         // the next iteration's bank of tile counters (used last by the previous iteration)
         for (int i = 0; i < kTileSlots; i++) ctl->tile_ctr[(ctl->iteration & 1) * kTileSlots + i] = 0;
+        ctl->heavy_n = 0;
+        ctl->heavy_ctr = 0;
     }
     if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
 }

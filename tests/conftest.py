@@ -43,4 +43,9 @@ def rows_digest(rows):
 # graph-program cases (make_golden.py's manifest); the generated analyses of
 # make_slog_golden.py have their own tests (test_wide.py)
 with open(os.path.join(GOLDEN, "manifest.json")) as _f:
-    GOLDEN_CASES = sorted(json.load(_f))
+    _ALL = sorted(json.load(_f))
+# the benchmark inputs (tc-er22, sg-tree15): minutes of CPU time on the reference and
+# the oracle, so they have their own GPU tests (test_scale_parity.py)
+LARGE_CASES = ("er4194304_tc", "tree32768_sg")
+GOLDEN_CASES = [c for c in _ALL if c not in LARGE_CASES]
+LARGE_GOLDEN = [c for c in _ALL if c in LARGE_CASES]

@@ -10,8 +10,15 @@ pairs, every relation's full count, a SHA-256 of each relation's sorted rows
 (data columns + intern id) and one of its data columns alone.  Small
 relations are also stored verbatim.
 
-Needs the reference tree (default /root/reference); run from the repo root:
-    python tests/golden/make_golden.py [--ref /root/reference]
+The LARGE cases are the benchmark's own inputs (transitive closure of the
+2^22-node Erdos-Renyi graph, same generation on the 2^15-node random tree);
+each takes minutes and gigabytes on one core, so they run only when named
+with --only.  Their records also carry the reference's fixpoint seconds and
+the driver's peak resident memory.
+
+Needs the reference tree, given by --ref or the RA_REFERENCE environment
+variable; run from the repo root:
+    RA_REFERENCE=<parallel-RA checkout> python tests/golden/make_golden.py [--only NAME ...]
 """
 from __future__ import annotations
 
@@ -19,10 +26,12 @@ import argparse
 import hashlib
 import json
 import os
+import resource
 import shutil
 import subprocess
 import sys
 import tempfile
+import time
 
 import numpy as np
 
@@ -42,6 +51,11 @@ CASES = [
     ("er20000_tc", "tc", ("er", 20000, 19000, 3)),
     ("tree256_sg", "sg", ("tree", 256, 11)),
     ("tree1024_sg", "sg", ("tree", 1024, 5)),
+]
+# the benchmark inputs: tc-er22 and sg-tree15 of bench.py
+LARGE_CASES = [
+    ("er4194304_tc", "tc", ("er", 1 << 22, 3984589, 2)),
+    ("tree32768_sg", "sg", ("tree", 1 << 15, 3)),
 ]
 VERBATIM_MAX_ROWS = 4096
 
@@ -65,7 +79,10 @@ def run_reference(prog, edge_path, work):
     empty = os.path.join(work, "empty_rel")
     P.datagen.write_empty_relation(empty)
     out = os.path.join(work, "out")
+    t0 = time.time()
     subprocess.run([DRIVER, prog, edge_path, empty, out], check=True, stdout=subprocess.DEVNULL)
+    wall = time.time() - t0
+    fixpoint = float(open(os.path.join(out, "time.txt")).read())
     hist = []
     for line in open(os.path.join(out, "history.txt")):
         a = line.split()
@@ -83,32 +100,47 @@ def run_reference(prog, edge_path, work):
                       "data_sha256": rows_digest(rows[:, :arity])}
         if count <= VERBATIM_MAX_ROWS:
             rels[name]["rows"] = rows.tolist()
-    return hist, rels
+    return hist, rels, fixpoint, wall
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("RA_REFERENCE"),
+                    help="parallel-RA checkout (default: $RA_REFERENCE)")
+    ap.add_argument("--only", nargs="*", help="run only these cases (LARGE cases run only when named)")
     args = ap.parse_args()
+    if not args.ref or not os.path.isdir(os.path.join(args.ref, "src")):
+        ap.error("give the reference tree with --ref or RA_REFERENCE")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}", "-j8"], check=True)
     for name in ("g5955", "g13236"):
         dst = os.path.join(HERE, f"{name}_edge_2_1_2")
         shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2"), dst)
         shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2.size"), dst + ".size")
-    manifest = {}
-    for name, prog, src in CASES:
+    mpath = os.path.join(HERE, "manifest.json")
+    manifest = json.load(open(mpath)) if os.path.exists(mpath) else {}
+    cases = CASES + LARGE_CASES
+    if args.only:
+        cases = [c for c in cases if c[0] in args.only]
+    else:
+        cases = CASES
+    for name, prog, src in cases:
         with tempfile.TemporaryDirectory() as work:
             rows = input_rows(src, args.ref)
             edge = os.path.join(work, "edge")
             P.datagen.write_relation(edge, rows)
-            hist, rels = run_reference(prog, edge, work)
+            hist, rels, fixpoint, wall = run_reference(prog, edge, work)
         case = {"program": prog, "source": list(src), "input_rows": int(rows.shape[0]),
                 "input_sha256": rows_digest(rows), "history": hist, "relations": rels}
+        if (name, prog, src) in LARGE_CASES:
+            case["reference_fixpoint_seconds_1core"] = round(fixpoint, 3)
+            case["reference_wall_seconds_1core"] = round(wall, 3)
+            case["reference_peak_rss_mb"] = round(resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss / 1024)
         with open(os.path.join(HERE, f"{name}.json"), "w") as f:
             json.dump(case, f, separators=(",", ":"))
         manifest[name] = {k: case[k] for k in ("program", "source", "input_rows")}
-        print(name, {r: v["count"] for r, v in rels.items()}, "iterations", [len(h[1]) for h in hist])
-    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+        print(name, {r: v["count"] for r, v in rels.items()}, "iterations", [len(h[1]) for h in hist],
+              "fixpoint %.1f s, wall %.1f s" % (fixpoint, wall), flush=True)
+    with open(mpath, "w") as f:
         json.dump(manifest, f, indent=1)
 
 
