@@ -13,8 +13,7 @@ the public C ABI from pinned host rows: upload, packing, fixed point and the
 read-back of the per-relation counts and the per-iteration history.
 
 ``--impl reference`` times the reference's own CPU code (oracle/_ref, the
-unchanged parallel-RA sources on a single-rank MPI stand-in) on a bounded
-sample of the same graph family; see DESIGN.md.
+unchanged parallel-RA sources on a single-rank MPI stand-in).
 
 Launch: ``python bench.py [--gpus N --steps K --warmup W]``; for N > 1 under
 torchrun, each rank runs its own seeded instance (instance-parallel replicas).

@@ -107,6 +107,8 @@ typedef struct ra_stats {
     uint64_t bitmap_relations;  /* output relations of device-driven SCCs that used a bitmap seen set */
     uint64_t persistent_launches; /* cooperative launches of the persistent SCC kernel (one per SCC run,
                                      plus one per replay after a buffer grew) */
+    uint64_t reach_sccs;        /* SCCs run by the reachability evaluator (composed reachable sets) */
+    double reach_ms;            /* host wall time of those evaluations (synchronised, launches included) */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose
@@ -296,11 +298,17 @@ int ra_relation_instance_summary(ra_program* p, int rel, uint64_t* counts, uint6
  * allocator).  dev_rows, dev_out_rows (room for nrows rows) and dev_out_nrows
  * are device pointers; stream is a cudaStream_t (0 = legacy default stream).
  * Returns RA_E_BADARG when nrows > RA_NOALLOC_MAX_ROWS.
+ * Returns RA_E_UNSUPPORTED when the rows' data columns do not pack into 63
+ * bits (arity x bits of the largest value).
  * Scratch is one fixed static device array (about 6 MB, held on every GPU
- * that loads the library until exit).  The first call on a device looks up
- * that array's device address, so make it before any stream capture on that
- * device.  All calls share the array: calls that overlap on the GPU (other
- * streams, other host threads) race and must be serialised by the caller. */
+ * that loads the library until exit).  Every call looks up that array's
+ * device address in the current context (no allocation); the first call on a
+ * device also loads the library's device code there, so make it before any
+ * stream capture on that device.  The call blocks the calling thread once (a
+ * stream synchronisation that reads the largest value back); the rest is
+ * stream-ordered, *dev_out_nrows included.  All calls share the array: calls
+ * that overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. */
 int ra_rows_distinct_noalloc(const uint64_t* dev_rows, uint64_t nrows, uint32_t arity,
                              uint64_t* dev_out_rows, uint64_t* dev_out_nrows, void* stream);
 

@@ -23,10 +23,18 @@ COPY, ACOPY, COPY_FILTER = 0, 1, 2
 _lib = None
 
 
+def reference_root() -> str | None:
+    """The parallel-RA checkout oracle/Makefile builds from ($RA_REFERENCE or its
+    default), or None when that tree is not on this machine."""
+    r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True)
+    path = r.stdout.strip()
+    return path if r.returncode == 0 and os.path.isdir(os.path.join(path, "src")) else None
+
+
 def build() -> None:
     """Compile the restatement (and, when the reference tree exists, oracle/_ref)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if os.path.isdir("/root/reference/src"):
+    if reference_root():
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"-j{os.cpu_count() or 4}"], check=True)
 
 

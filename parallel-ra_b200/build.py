@@ -56,7 +56,9 @@ def build_cxx(force=False):
               f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN"])
 
 
-REFERENCE = os.environ.get("RA_REFERENCE", "/root/reference")
+# the parallel-RA checkout whose program sources are compiled against cxx/src
+# (given by the caller; without it the binaries already in cxx/bin/ are used)
+REFERENCE = os.environ.get("RA_REFERENCE", "")
 BIN_DIR = os.path.join(CXX_DIR, "bin")
 
 
@@ -71,6 +73,8 @@ def build_reference_programs(force=False):
     cxx/src/parallel_RA_inc.h; nothing is copied.  Only possible where the
     reference tree exists; the binaries in cxx/bin/ are used elsewhere.
     """
+    if not REFERENCE:
+        return
     progs = {"TC": os.path.join(REFERENCE, "tests", "transitive_closure.cpp")}
     for name in GENERATED_PROGRAMS:   # the reference's generated analyses (wide tuples)
         progs[name] = os.path.join(REFERENCE, "tests", name + ".cpp")

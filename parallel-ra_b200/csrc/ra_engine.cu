@@ -18,6 +18,7 @@
 #include "../../include/ra_engine.h"
 #include "ra_dense.cuh"
 #include "ra_persist.cuh"
+#include "ra_reach.cuh"
 #include "ra_wide.cuh"
 
 #include <algorithm>
@@ -239,6 +240,8 @@ struct ra_program {
     std::vector<u64> bmt_bases;      // the instance bases the tables were built for
     bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
     bool use_persist = false;     // RA_PERSIST=1: the persistent SCC kernel instead of CUDA-graph iterations
+    bool use_reach = true;        // RA_NO_REACH=1: the semi-naive loop for closure-shaped SCCs too
+    u64 reach_arena_hint = 0;     // arena entries the last reachability evaluation used
     bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
 
@@ -1905,6 +1908,52 @@ struct DenseBufs {
     }
 };
 
+// The end of a closure-shaped SCC run by an evaluator that is not the iteration
+// loop (dense rows, composed reachable sets): `total` new tuples already written
+// after R's `n_stored` stored ones, lv[k] of them new in iteration k (k < L),
+// `iterations` iterations in all (the last finds nothing).  Records the same
+// per-iteration history as the semi-naive bookkeeping (end_of_iteration,
+// RAM::check_for_fixed_point, src/RAM/RA_tasks.cpp:1072-1085) and leaves R as the
+// loop would: every tuple in its full version.
+void finish_closure_scc(ra_program* p, Scc& s, int out, Relation& R, u64 n_stored, u64 total,
+                        const std::vector<u64>& lv, u64 L, u64 iterations)
+{
+    std::vector<u64> f(s.rels.size()), d(s.rels.size());
+    for (size_t i = 0; i < s.rels.size(); i++) {
+        f[i] = p->rels[s.rels[i]].full_n;
+        d[i] = p->rels[s.rels[i]].delta_n;
+    }
+    std::vector<uint64_t> hist;
+    for (u64 k = 0; k < iterations; k++) {
+        u64 sd = 0, sf = 0;
+        for (size_t i = 0; i < s.rels.size(); i++) {
+            f[i] += d[i];
+            d[i] = (s.rels[i] == out && k < L) ? lv[k] : 0;
+            sd += d[i];
+            sf += f[i];
+        }
+        hist.push_back(sd);
+        hist.push_back(sf);
+    }
+    p->history.push_back((uint64_t)s.id);
+    p->history.push_back(iterations);
+    p->history.insert(p->history.end(), hist.begin(), hist.end());
+
+    // the log is [old full | old delta | new]: sorted only when a single sorted region holds it all
+    const bool sorted = total == 0 && ((R.delta_n == 0 && R.full_sorted) || (R.full_n == 0 && R.delta_sorted));
+    intern_counter(p, R.tag) += total;
+    R.full_n = n_stored + total;
+    R.delta_n = 0;
+    R.newt_n = 0;
+    R.full_sorted = sorted;
+    R.delta_sorted = true;
+    R.full_version = fresh_stamp();
+    R.delta_version = fresh_stamp();
+    if (R.seen) R.seen_dirty = true;   // the hash set holds none of the new tuples
+    p->stats.iterations += iterations;
+    p->stats.new_tuples += total;
+}
+
 // Runs SCC s with the dense row-closure evaluator (ra_dense.cuh) when its one
 // rule has the transitive-closure shape and the bit matrices fit the tuned
 // budget; returns false (nothing done) otherwise.  Leaves the SCC's relations
@@ -2152,43 +2201,294 @@ bool run_scc_dense(ra_program* p, Scc& s)
         CK(cudaStreamSynchronize(p->stream));
     }
 
-    // history: the semi-naive bookkeeping of every iteration (end_of_iteration's)
-    std::vector<u64> f(s.rels.size()), d(s.rels.size());
-    for (size_t i = 0; i < s.rels.size(); i++) {
-        f[i] = p->rels[s.rels[i]].full_n;
-        d[i] = p->rels[s.rels[i]].delta_n;
-    }
-    std::vector<uint64_t> hist;
-    for (u64 k = 0; k < iterations; k++) {
-        u64 sd = 0, sf = 0;
-        for (size_t i = 0; i < s.rels.size(); i++) {
-            f[i] += d[i];
-            d[i] = (s.rels[i] == ru.out && k < L) ? lv[k] : 0;
-            sd += d[i];
-            sf += f[i];
-        }
-        hist.push_back(sd);
-        hist.push_back(sf);
-    }
-    p->history.push_back((uint64_t)s.id);
-    p->history.push_back(iterations);
-    p->history.insert(p->history.end(), hist.begin(), hist.end());
-
-    // the log is [old full | old delta | new]: sorted only when a single sorted region holds it all
-    const bool sorted = total == 0 && ((R.delta_n == 0 && R.full_sorted) || (R.full_n == 0 && R.delta_sorted));
-    ctr += total;
-    R.full_n = n_stored + total;
-    R.delta_n = 0;
-    R.newt_n = 0;
-    R.full_sorted = sorted;
-    R.delta_sorted = true;
-    R.full_version = fresh_stamp();
-    R.delta_version = fresh_stamp();
-    if (R.seen) R.seen_dirty = true;   // the hash set holds none of the new tuples
-    p->stats.iterations += iterations;
-    p->stats.new_tuples += total;
+    finish_closure_scc(p, s, ru.out, R, n_stored, total, lv, L, iterations);
     p->stats.join_candidates += cnt[1];
     p->stats.dense_sccs++;
+    return true;
+}
+
+// Device buffers of one reachability evaluation, freed on every exit.
+struct ReachBufs {
+    ra_program* p;
+    u32 *sval = nullptr, *indeg = nullptr, *rpar = nullptr, *rem = nullptr, *queue = nullptr, *seg_len = nullptr;
+    u32* flags = nullptr;
+    u64 *rcsr = nullptr, *ctr = nullptr, *seg_off = nullptr, *row_new = nullptr, *row_off = nullptr;
+    u64 *level_total = nullptr, *arena = nullptr;
+    u32* cyc = nullptr;
+    u64* cyc_n = nullptr;
+    u64 *c_soff = nullptr, *c_singles = nullptr, *c_xoff = nullptr;
+    u32 *c_node = nullptr, *c_xnode = nullptr, *c_xdist = nullptr;
+    explicit ReachBufs(ra_program* pp) : p(pp) {}
+    ~ReachBufs()
+    {
+        for (u32** q : {&sval, &indeg, &rpar, &rem, &queue, &seg_len, &flags, &cyc, &c_node, &c_xnode, &c_xdist})
+            dev_free(p, q);
+        for (u64** q : {&rcsr, &ctr, &seg_off, &row_new, &row_off, &level_total, &arena, &cyc_n, &c_soff, &c_singles,
+                        &c_xoff})
+            dev_free(p, q);
+    }
+};
+
+constexpr u64 kReachLevels = 1ull << kDistBits;   // distances fit 16 bits
+
+// Runs SCC s with the reachability evaluator (ra_reach.cuh) when its one rule has
+// the transitive-closure shape and R's stored tuples are exactly S reversed;
+// returns false (nothing done) otherwise, or when the graph is mostly cyclic or
+// too deep for 16-bit distances (the semi-naive loop runs it instead).  Leaves
+// the relations and the per-iteration history as the semi-naive loop would.
+bool run_scc_reach(ra_program* p, Scc& s)
+{
+    if (!p->use_reach || !s.fixpoint || s.rules.size() != 1 || s.rules[0].kind != kJoin) return false;
+    if (p->id_order != RA_IDS_EMISSION || p->batch_size != 1 || p->cp_every || p->n_inst) return false;
+    const Rule& ru = s.rules[0];
+    const JoinPlan jp = make_join_plan(p, ru);
+    if (jp.outer_rel != ru.out || jp.outer_ver != RA_DELTA || jp.inner_ver != RA_FULL || jp.inner_rel == ru.out)
+        return false;
+    Relation& R = p->rels[ru.out];
+    Relation& S = p->rels[jp.inner_rel];
+    if (R.arity != 2 || S.arity != 2 || R.jcc != 1) return false;
+    const Projection& pj = jp.pj;
+    if (pj.n != 2 || pj.side[0] != 1 || pj.col[0] != 1 || pj.side[1] != 0 || pj.col[1] != 1) return false;
+    if (std::find(s.rels.begin(), s.rels.end(), jp.inner_rel) != s.rels.end() && S.delta_n != 0) return false;
+    if (R.full_n != 0 || !R.keys_unique || !S.keys_unique || p->bits > 31) return false;
+    const u64 *sk, *sv;
+    u64 sn;
+    version_rows(p, S, RA_FULL, &sk, &sv, &sn);
+    if (R.delta_n != sn || sn == 0) return false;
+    const u64 n = p->max_value + 1;
+    if (n > 16 * sn + (1u << 16)) return false;   // a sparse value domain: per-value arrays would dwarf the input
+    const u64* scsr = version_csr(p, S, RA_FULL);
+
+    ReachBufs B(p);
+    dev_alloc(p, &B.sval, sn);
+    dev_alloc(p, &B.indeg, n + 1);
+    dev_alloc(p, &B.rcsr, n + 1);
+    dev_alloc(p, &B.rpar, sn);
+    dev_alloc(p, &B.rem, n);
+    dev_alloc(p, &B.queue, n);
+    dev_alloc(p, &B.seg_len, n);
+    dev_alloc(p, &B.seg_off, n);
+    dev_alloc(p, &B.ctr, 8);
+    dev_alloc(p, &B.flags, 1);
+    // predecessor lists (a counting sort of S by column 1)
+    CK(cudaMemsetAsync(B.indeg, 0, (n + 1) * 4, p->stream));
+    reach_sval_kernel<<<grid_for(sn), kThreads, 0, p->stream>>>(sk, sn, p->bits, B.sval, B.indeg);
+    LAUNCHED();
+    scan_exclusive<u32>(p, B.indeg, n + 1, B.rcsr, false);
+    CK(cudaMemsetAsync(B.indeg, 0, (n + 1) * 4, p->stream));
+    reach_parents_kernel<<<grid_for(sn), kThreads, 0, p->stream>>>(sk, sn, p->bits, B.rcsr, B.indeg, B.rpar);
+    LAUNCHED();
+    ReachArgs a{};
+    a.n = n;
+    a.scsr = scsr;
+    a.sval = B.sval;
+    a.rcsr = B.rcsr;
+    a.rpar = B.rpar;
+    a.rem = B.rem;
+    a.queue = B.queue;
+    a.ctr = B.ctr;
+    a.seg_off = B.seg_off;
+    a.seg_len = B.seg_len;
+    a.flags = B.flags;
+    // R's stored tuples must be exactly S reversed (equal counts, distinct, each one found)
+    CK(cudaMemsetAsync(B.flags, 0, 4, p->stream));
+    reach_check_kernel<<<grid_for(R.delta_n), kThreads, 0, p->stream>>>(a, R.keys, R.delta_n, p->bits);
+    LAUNCHED();
+    u32 fl = 0;
+    CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    if (fl & kReachMismatch) return false;
+
+    static int occ = 0, sms = 0;
+    if (!occ) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reach_dataflow_kernel, kThreads, 0));
+        if (occ < 1) fail(p, RA_E_CUDA, "the reachability kernel does not fit on an SM");
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    u64 cap = std::max<u64>(p->reach_arena_hint, 24 * sn + (1u << 20));
+    std::vector<u64> hc(8);
+    for (;;) {
+        dev_free(p, &B.arena);
+        dev_alloc(p, &B.arena, cap);
+        a.arena = B.arena;
+        a.arena_cap = cap;
+        CK(cudaMemsetAsync(B.ctr, 0, 8 * 8, p->stream));
+        CK(cudaMemsetAsync(B.flags, 0, 4, p->stream));
+        reach_init_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a);
+        LAUNCHED();
+        reach_sinks_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a);
+        LAUNCHED();
+        void* args[] = {&a};
+        CK(cudaLaunchCooperativeKernel((const void*)reach_dataflow_kernel, dim3(sms * occ), dim3(kThreads), args, 0,
+                                       p->stream));
+        LAUNCHED();
+        CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaMemcpyAsync(hc.data(), B.ctr, 8 * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        if (fl & kReachTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a bounded wait of the reachability evaluator gave up", s.id);
+        if (fl & kReachArena) {   // room for what it asked, and some
+            cap = std::max<u64>(2 * cap, hc[3] + hc[3] / 4);
+            p->stats.regrows++;
+            continue;
+        }
+        break;
+    }
+    if (fl & kReachDepth) return false;
+    // nodes that reach a cycle: searched on the host over that part of the graph
+    const u64 finished = hc[2];
+    if (finished < n) {
+        const u64 U = n - finished;
+        if (U > std::max<u64>(1u << 16, n / 64)) return false;   // mostly cyclic: the semi-naive loop
+        dev_alloc(p, &B.cyc, U);
+        dev_alloc(p, &B.cyc_n, 1);
+        CK(cudaMemsetAsync(B.cyc_n, 0, 8, p->stream));
+        reach_cyclic_list_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a, B.cyc, B.cyc_n, U);
+        LAUNCHED();
+        std::vector<u32> cyc(U);
+        CK(cudaMemcpyAsync(cyc.data(), B.cyc, U * 4, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        std::sort(cyc.begin(), cyc.end());
+        // successors of those nodes (S's rows are the CSR ranges), gathered on the device
+        CK(cudaMemcpyAsync(B.cyc, cyc.data(), U * 4, cudaMemcpyHostToDevice, p->stream));
+        dev_alloc(p, &B.c_soff, 2 * U);
+        reach_gather_ranges_kernel<<<grid_for(U), kThreads, 0, p->stream>>>(scsr, B.cyc, U, B.c_soff);
+        LAUNCHED();
+        std::vector<u64> lohi(2 * U), off(U + 1);
+        CK(cudaMemcpyAsync(lohi.data(), B.c_soff, 2 * U * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaStreamSynchronize(p->stream));
+        off[0] = 0;
+        for (u64 i = 0; i < U; i++) off[i + 1] = off[i] + (lohi[2 * i + 1] - lohi[2 * i]);
+        std::vector<u32> succ(off[U]);
+        if (off[U]) {
+            dev_alloc(p, &B.c_xoff, U + 1);
+            dev_alloc(p, &B.c_xnode, off[U]);
+            CK(cudaMemcpyAsync(B.c_xoff, off.data(), (U + 1) * 8, cudaMemcpyHostToDevice, p->stream));
+            reach_gather_succ_kernel<<<std::max<u64>(1, std::min<u64>((U + kWarps - 1) / kWarps, (u64)kSms * 8)),
+                                       kThreads, 0, p->stream>>>(B.sval, B.c_soff, B.c_xoff, U, B.c_xnode);
+            LAUNCHED();
+            CK(cudaMemcpyAsync(succ.data(), B.c_xnode, off[U] * 4, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+            dev_free(p, &B.c_xoff);
+            dev_free(p, &B.c_xnode);
+        }
+        dev_free(p, &B.c_soff);
+        auto index_of = [&](u32 v) -> long {
+            auto it = std::lower_bound(cyc.begin(), cyc.end(), v);
+            return (it != cyc.end() && *it == v) ? (long)(it - cyc.begin()) : -1;
+        };
+        // per node: a breadth-first search over the nodes that reach a cycle, recording the
+        // cycle-free nodes met first (their own sets are complete) with their distances
+        std::vector<u64> soff(1, 0), singles, xoff(1, 0);
+        std::vector<u32> xnode, xdist;
+        std::vector<u32> dist(U, 0), seen(U, 0);
+        std::vector<u32> frontier, next;
+        std::unordered_map<u32, u32> exits;
+        u32 stamp = 0;
+        for (u64 i = 0; i < U; i++) {
+            ++stamp;
+            exits.clear();
+            frontier.assign(1, (u32)i);
+            std::vector<std::pair<u32, u32>> found;   // (value, distance)
+            for (u32 d = 1; !frontier.empty(); d++) {
+                if (d >= kReachLevels) return false;
+                next.clear();
+                for (u32 ui : frontier)
+                    for (u64 e = off[ui]; e < off[ui + 1]; e++) {
+                        const u32 w = succ[e];
+                        const long wi = index_of(w);
+                        if (wi < 0) {
+                            auto it = exits.find(w);
+                            if (it == exits.end()) exits.emplace(w, d);
+                            continue;
+                        }
+                        if (seen[wi] == stamp) continue;
+                        seen[wi] = stamp;
+                        dist[wi] = d;
+                        found.push_back({w, d});
+                        if ((u64)wi != i) next.push_back((u32)wi);
+                    }
+                frontier.swap(next);
+            }
+            std::vector<std::pair<u32, u32>> ex(exits.begin(), exits.end());
+            std::sort(ex.begin(), ex.end());
+            for (auto& e : ex) found.push_back(e);
+            std::sort(found.begin(), found.end());
+            for (auto& f : found) singles.push_back(((u64)f.first << kDistBits) | f.second);
+            soff.push_back(singles.size());
+            for (auto& e : ex) {
+                xnode.push_back(e.first);
+                xdist.push_back(e.second);
+            }
+            xoff.push_back(xnode.size());
+        }
+        dev_alloc(p, &B.c_node, U);
+        dev_alloc(p, &B.c_soff, U + 1);   // (freed above after the gather)
+        dev_alloc(p, &B.c_singles, std::max<size_t>(singles.size(), 1));
+        dev_alloc(p, &B.c_xoff, U + 1);
+        dev_alloc(p, &B.c_xnode, std::max<size_t>(xnode.size(), 1));
+        dev_alloc(p, &B.c_xdist, std::max<size_t>(xdist.size(), 1));
+        CK(cudaMemcpyAsync(B.c_node, cyc.data(), U * 4, cudaMemcpyHostToDevice, p->stream));
+        CK(cudaMemcpyAsync(B.c_soff, soff.data(), (U + 1) * 8, cudaMemcpyHostToDevice, p->stream));
+        if (!singles.empty())
+            CK(cudaMemcpyAsync(B.c_singles, singles.data(), singles.size() * 8, cudaMemcpyHostToDevice, p->stream));
+        CK(cudaMemcpyAsync(B.c_xoff, xoff.data(), (U + 1) * 8, cudaMemcpyHostToDevice, p->stream));
+        if (!xnode.empty()) {
+            CK(cudaMemcpyAsync(B.c_xnode, xnode.data(), xnode.size() * 4, cudaMemcpyHostToDevice, p->stream));
+            CK(cudaMemcpyAsync(B.c_xdist, xdist.data(), xdist.size() * 4, cudaMemcpyHostToDevice, p->stream));
+        }
+        ReachCyclic c{B.c_node, B.c_soff, B.c_singles, B.c_xoff, B.c_xnode, B.c_xdist, U};
+        for (;;) {
+            CK(cudaMemsetAsync(B.flags, 0, 4, p->stream));
+            reach_cyclic_kernel<<<std::max<u64>(1, std::min<u64>((U + kWarps - 1) / kWarps, (u64)kSms * 4)), kThreads, 0,
+                                  p->stream>>>(a, c);
+            LAUNCHED();
+            CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaMemcpyAsync(hc.data(), B.ctr, 8 * 8, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+            if (fl & kReachDepth) return false;
+            if (!(fl & kReachArena)) break;
+            // a larger arena, keeping what the cycle-free nodes wrote
+            const u64 ncap = std::max<u64>(2 * cap, hc[3] + hc[3] / 4);
+            u64* na;
+            dev_alloc(p, &na, ncap);
+            CK(cudaMemcpyAsync(na, B.arena, cap * 8, cudaMemcpyDeviceToDevice, p->stream));
+            dev_free(p, &B.arena);
+            B.arena = na;
+            a.arena = na;
+            a.arena_cap = cap = ncap;
+            p->stats.regrows++;
+            // the failed launch's allocations are past the old end: nothing it wrote is kept
+            CK(cudaMemcpyAsync(B.ctr + 3, &hc[3], 8, cudaMemcpyHostToDevice, p->stream));
+        }
+    }
+    p->reach_arena_hint = std::max<u64>(p->reach_arena_hint, hc[3] + hc[3] / 8);
+
+    // new tuples, row by row, after R's stored ones
+    dev_alloc(p, &B.row_new, n);
+    dev_alloc(p, &B.row_off, n);
+    reach_count_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a, B.row_new);
+    LAUNCHED();
+    const u64 total = scan_exclusive<u64>(p, B.row_new, n, B.row_off);
+    const u64 n_stored = R.full_n + R.delta_n;
+    ensure_log(p, R, n_stored + total);
+    dev_alloc(p, &B.level_total, kReachLevels + 1);
+    CK(cudaMemsetAsync(B.level_total, 0, (kReachLevels + 1) * 8, p->stream));
+    reach_emit_kernel<<<std::min<u64>((n + kWarps - 1) / kWarps, (u64)kSms * 16), kThreads, 0, p->stream>>>(
+        a, B.row_off, p->bits, R.keys + n_stored, R.ids + n_stored, (u64)R.tag << 46, intern_counter(p, R.tag),
+        B.level_total, kReachLevels, B.level_total + kReachLevels);
+    LAUNCHED();
+    std::vector<u64> lv(kReachLevels + 1);
+    CK(cudaMemcpyAsync(lv.data(), B.level_total, (kReachLevels + 1) * 8, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    p->stats.reach_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    u64 L = 0;
+    while (L < kReachLevels && lv[L]) L++;
+    p->stats.join_candidates += lv[kReachLevels];   // what the semi-naive loop's joins would have produced
+    finish_closure_scc(p, s, ru.out, R, n_stored, total, lv, L, L + 1);
+    p->stats.reach_sccs++;
     return true;
 }
 
@@ -2225,7 +2525,7 @@ void run_scc(ra_program* p, Scc& s)
         for (size_t i = 0; i < s.rels.size(); i++)
             if (s.init[i]) full_to_delta(p, p->rels[s.rels[i]]);
     }
-    if (run_scc_dense(p, s)) {
+    if (run_scc_dense(p, s) || run_scc_reach(p, s)) {
         p->pending_merge = s.rels;
         return;
     }
@@ -2536,6 +2836,7 @@ int ra_program_create(int device, ra_program** out)
         CK(cudaMallocHost(&p->hctl, sizeof(IterCtl)));
         if (const char* e = getenv("RA_NO_GRAPH")) p->use_graphs = atoi(e) == 0;
         if (const char* e = getenv("RA_PERSIST")) p->use_persist = atoi(e) != 0;
+        if (const char* e = getenv("RA_NO_REACH")) p->use_reach = atoi(e) == 0;
         if (const char* e = getenv("RA_KERNEL_EVENTS")) p->kernel_events = atoi(e) != 0;
     });
     if (st != RA_OK) {

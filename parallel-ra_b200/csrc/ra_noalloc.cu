@@ -13,13 +13,12 @@
 // All scratch lives in one file-scope __device__ array of fixed size
 // (kNoallocBytes below); every GPU that loads this library keeps that much
 // memory reserved until the process exits.  The entry point launches kernels,
-// memsets, copies and a stream synchronisation -- nothing that allocates.
+// memsets, copies and one stream synchronisation (to read the largest value,
+// which sets the packing width) -- nothing that allocates.
 #include "../../include/ra_engine.h"
 #include "ra_kernels.cuh"
 
 #include <utility>
-
-#include <mutex>
 
 using namespace ra;
 
@@ -44,24 +43,34 @@ constexpr u64 kNoallocBytes = kWords * 8;   // about 6 MB
 static_assert(kNoallocBytes < (7u << 20), "no-alloc scratch stays modest");
 
 // The scratch.  Host code must not use this name as an address: its device
-// address comes from cudaGetSymbolAddress, once per device (see scratch_for).
+// address comes from cudaGetSymbolAddress (see scratch_for).
 static __device__ __align__(256) u64 g_noalloc_scratch[kWords];
 
-std::mutex g_setup_mutex;
-u64* g_scratch_ptr[64] = {};
-
-// Device address of the scratch on the current device, looked up on first use.
-int scratch_for(int dev, u64** out)
+// Device address of the scratch in the calling thread's current context.  Looked
+// up on every call (the lookup allocates nothing), so an address never outlives
+// the context it belongs to -- a device reset or another context on the same
+// device gets its own.
+int scratch_for(u64** out)
 {
-    if (dev < 0 || dev >= 64) return RA_E_BADARG;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RA_E_CUDA;
-        g_scratch_ptr[dev] = (u64*)p;
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RA_E_CUDA;
+    *out = (u64*)p;
     return RA_OK;
+}
+
+// rows_unpack for a row count that stays on the device
+__global__ void __launch_bounds__(kThreads) unpack_counted_kernel(const u64* __restrict__ keys,
+                                                                  const u64* __restrict__ ids,
+                                                                  const u64* __restrict__ count, int arity, int bits,
+                                                                  u64* __restrict__ rows)
+{
+    const u64 n = *count;
+    const int w = arity + 1;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads) {
+        const u64 k = keys[i];
+        for (int c = 0; c < arity; c++) rows[i * w + c] = column_of(k, arity, c, bits);
+        rows[i * w + arity] = ids[i];
+    }
 }
 
 int blocks_for(u64 n)
@@ -133,11 +142,9 @@ extern "C" int ra_rows_distinct_noalloc(const uint64_t* dev_rows_in, uint64_t nr
     u64* dev_out_nrows = (u64*)dev_out_nrows_in;
     if (nrows > kMaxRows || arity == 0 || arity > 8) return RA_E_BADARG;
     if ((nrows && (!dev_rows || !dev_out_rows)) || !dev_out_nrows) return RA_E_BADARG;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return RA_E_CUDA;
     Ctx c;
     c.st = (cudaStream_t)stream;
-    int st = scratch_for(dev, &c.s);
+    int st = scratch_for(&c.s);
     if (st != RA_OK) return st;
     if (nrows == 0) {
         c.ck(cudaMemsetAsync(dev_out_nrows, 0, 8, c.st));
@@ -169,12 +176,9 @@ extern "C" int ra_rows_distinct_noalloc(const uint64_t* dev_rows_in, uint64_t nr
     scan<u32>(c, flag, nrows, rank);
     compact_flagged<<<blocks_for(nrows), kThreads, 0, c.st>>>(ka, va, flag, rank, nrows, kb, vb);
     copy_count_kernel<<<1, 1, 0, c.st>>>(c.s + kOffScalar, dev_out_nrows);
-    c.ck(cudaGetLastError());
-    c.ck(cudaMemcpyAsync(hostv, c.s + kOffScalar, 8, cudaMemcpyDeviceToHost, c.st));
-    c.ck(cudaStreamSynchronize(c.st));
-    if (c.err != cudaSuccess) return RA_E_CUDA;
-    const u64 m = hostv[0];
-    rows_unpack<<<blocks_for(m), kThreads, 0, c.st>>>(kb, vb, m, (int)arity, bits, dev_out_rows);
+    // the distinct rows stay stream-ordered: the count is read on the device
+    unpack_counted_kernel<<<blocks_for(nrows), kThreads, 0, c.st>>>(kb, vb, c.s + kOffScalar, (int)arity, bits,
+                                                                     dev_out_rows);
     c.ck(cudaGetLastError());
     return c.err == cudaSuccess ? RA_OK : RA_E_CUDA;
 }

@@ -55,7 +55,7 @@ class Stats(C.Structure):
         ("graph_build_ms", C.c_double), ("regrows", C.c_uint64), ("device_bytes", C.c_uint64),
         ("device_bytes_peak", C.c_uint64), ("dense_sccs", C.c_uint64), ("dense_search_ms", C.c_double),
         ("dense_emit_ms", C.c_double), ("bitmap_relations", C.c_uint64),
-        ("persistent_launches", C.c_uint64),
+        ("persistent_launches", C.c_uint64), ("reach_sccs", C.c_uint64), ("reach_ms", C.c_double),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 

@@ -16,9 +16,9 @@ each takes minutes and gigabytes on one core, so they run only when named
 with --only.  Their records also carry the reference's fixpoint seconds and
 the driver's peak resident memory.
 
-Needs the reference tree, given by --ref or the RA_REFERENCE environment
-variable; run from the repo root:
-    RA_REFERENCE=<parallel-RA checkout> python tests/golden/make_golden.py [--only NAME ...]
+Needs the reference tree: --ref, or oracle/Makefile's default (which the
+RA_REFERENCE environment variable overrides); run from the repo root:
+    python tests/golden/make_golden.py [--ref <parallel-RA checkout>] [--only NAME ...]
 """
 from __future__ import annotations
 
@@ -39,6 +39,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 import parallel_ra_b200 as P  # noqa: E402
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
 
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 
@@ -105,8 +107,8 @@ def run_reference(prog, edge_path, work):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("RA_REFERENCE"),
-                    help="parallel-RA checkout (default: $RA_REFERENCE)")
+    ap.add_argument("--ref", default=O.reference_root(),
+                    help="parallel-RA checkout (default: oracle/Makefile's, $RA_REFERENCE)")
     ap.add_argument("--only", nargs="*", help="run only these cases (LARGE cases run only when named)")
     args = ap.parse_args()
     if not args.ref or not os.path.isdir(os.path.join(args.ref, "src")):

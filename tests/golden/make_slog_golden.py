@@ -1,6 +1,7 @@
 """Golden vectors of the reference's generated analyses (wide tuples).
 
-For each program below, from the reference tree (default /root/reference):
+For each program below, from the reference tree (--ref, or oracle/Makefile's
+default, which $RA_REFERENCE overrides):
   * parses tests/<program>.cpp -- generated code with one statement per
     relation, SCC, rule and dependency -- into a program description
     tests/golden/<program>/program.txt (format in oracle/programs.h);
@@ -16,7 +17,7 @@ For each program below, from the reference tree (default /root/reference):
 
 The copy_filter lambdas are recognised from their text (comparisons of
 columns 0 and 1).  Run from the repo root:
-    python tests/golden/make_slog_golden.py [--ref /root/reference]
+    python tests/golden/make_slog_golden.py [--ref <parallel-RA checkout>]
 """
 from __future__ import annotations
 
@@ -37,6 +38,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 import parallel_ra_b200 as P  # noqa: E402
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
 
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 PROGRAMS = ["cfa-4-4-64", "worstcase-110-terms-4-m"]
@@ -164,7 +167,8 @@ def printed_sizes(prog: str, ref: str, data_dir: str, work: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=O.reference_root(),
+                    help="parallel-RA checkout (default: oracle/Makefile's, $RA_REFERENCE)")
     ap.add_argument("programs", nargs="*", default=PROGRAMS)
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}", "-j8"], check=True)

@@ -6,6 +6,7 @@
   through the C++ classes and must reproduce the golden history and rows.
 """
 import os
+import runpy
 import subprocess
 
 import numpy as np
@@ -112,26 +113,33 @@ def test_cxx_api_matches_goldens(tmp_path, name, id_order):
             assert rows_digest(np.ascontiguousarray(got[:, :-1])) == exp["data_sha256"], rname
 
 
-@pytest.mark.gpu
-def test_integration_ctypes_snippet_runs(tmp_path):
-    """The ctypes example in INTEGRATION.md computes TC of a 2-edge chain (3 pairs)."""
+def _python_blocks():
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    block = text.split("```python", 1)[1].split("```", 1)[0]
-    env = {}
+    return [b.split("```", 1)[0].lstrip("\n") for b in text.split("```python")[1:]]
+
+
+def test_integration_md_quotes_the_example_files():
+    """INTEGRATION.md's Python examples are these test files, verbatim."""
+    blocks = _python_blocks()
+    for name in ("integration_ctypes_example.py", "integration_batch_example.py"):
+        with open(os.path.join(ROOT, "tests", name)) as f:
+            assert f.read() in blocks, name
+
+
+@pytest.mark.gpu
+def test_integration_ctypes_example_runs():
+    """The ctypes example (quoted in INTEGRATION.md) computes TC of a 2-edge chain (3 pairs)."""
     cwd = os.getcwd()
     os.chdir(ROOT)
     try:
-        exec(compile(block, "INTEGRATION.md", "exec"), env)
+        env = runpy.run_path(os.path.join(ROOT, "tests", "integration_ctypes_example.py"))
     finally:
         os.chdir(cwd)
     assert env["f"].value == 3
 
 
 @pytest.mark.gpu
-def test_integration_batch_snippet_runs():
-    """The batching example in INTEGRATION.md runs and its assertion holds."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    block = text.split("```python")[2].split("```", 1)[0]
-    env = {}
-    exec(compile(block, "INTEGRATION.md", "exec"), env)
+def test_integration_batch_example_runs():
+    """The batching example (quoted in INTEGRATION.md) runs and its assertion holds."""
+    env = runpy.run_path(os.path.join(ROOT, "tests", "integration_batch_example.py"))
     assert len(env["results"]) == 3

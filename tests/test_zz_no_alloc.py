@@ -65,3 +65,25 @@ def test_noalloc_matches_relation_loading_twice_in_a_row():
         got = distinct_noalloc(rows, arity)
         assert got.shape == want.shape
         assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_noalloc_zero_rows_and_unpackable_rows():
+    import torch
+    L = P.engine.lib()
+    out = torch.full((4, 3), -7, dtype=torch.int64, device="cuda")
+    n = torch.full((1,), 99, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    assert L.ra_rows_distinct_noalloc(None, 0, 2, out.data_ptr(), n.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert int(n.item()) == 0
+    assert bool((out == -7).all())   # nothing written
+    # three columns of values near 2^40 need 3 x 41 bits: more than one packed key holds
+    rows = np.array([[1 << 40, 1, 2, 0], [3, 1 << 40, 5, 1]], dtype=np.uint64)
+    dev_in = torch.from_numpy(rows.view(np.int64)).cuda()
+    torch.cuda.synchronize()
+    st = L.ra_rows_distinct_noalloc(dev_in.data_ptr(), 2, 3, out.data_ptr(), n.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert st == 5   # RA_E_UNSUPPORTED
+    assert bool((out == -7).all())
+
