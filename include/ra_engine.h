@@ -108,7 +108,10 @@ typedef struct ra_stats {
     uint64_t persistent_launches; /* cooperative launches of the persistent SCC kernel (one per SCC run,
                                      plus one per replay after a buffer grew) */
     uint64_t reach_sccs;        /* SCCs run by the reachability evaluator (composed reachable sets) */
+    uint64_t reach_levels;      /* levels it swept (longest path over nodes that reach no cycle, + 1) */
     double reach_ms;            /* host wall time of those evaluations (synchronised, launches included) */
+    double reach_phase_ms[4];   /* of which: [0] graph set-up and checks, [1] the level sweep,
+                                   [2] nodes that reach a cycle, [3] emission of the new tuples */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose
@@ -186,6 +189,16 @@ int ra_program_set_id_order(ra_program* p, int mode);
  * graph.  A profiling aid: the reference's counterpart is the per-phase
  * MPI_Wtime table of RAM::execute_in_batches (src/RAM/RA_tasks.cpp:1138-1253). */
 int ra_program_set_launch_timing(ra_program* p, int on);
+/* No counterpart in the reference (whose only evaluator is the semi-naive loop
+ * of RAM::execute_in_batches).  Chooses how the engine runs its SCCs, with the
+ * same results either way:
+ *   reach       closure-shaped SCCs (R(z,x) :- R_delta(y,x), S_full(y,z), R
+ *               initially S reversed) by composing reachable sets (default 0;
+ *               RA_REACH=1 in the environment sets 1 at creation);
+ *   persistent  every other device-driven SCC as one cooperative launch of the
+ *               persistent iteration kernel instead of a CUDA graph of
+ *               per-iteration launches (default 0; RA_PERSIST=1 sets 1). */
+int ra_program_set_evaluators(ra_program* p, int reach, int persistent);
 
 /* relation(jcc, is_canonical, arity, tag, name, file, version),
  * src/relation/balanced_hash_relation.h:97.  0 <= jcc <= arity <= 63.  A program

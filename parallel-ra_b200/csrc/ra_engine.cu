@@ -240,7 +240,7 @@ struct ra_program {
     std::vector<u64> bmt_bases;      // the instance bases the tables were built for
     bool use_graphs = true;       // RA_NO_GRAPH=1: replay the iteration from the host instead
     bool use_persist = false;     // RA_PERSIST=1: the persistent SCC kernel instead of CUDA-graph iterations
-    bool use_reach = true;        // RA_NO_REACH=1: the semi-naive loop for closure-shaped SCCs too
+    bool use_reach = false;       // RA_REACH=1: closure-shaped SCCs by composing reachable sets
     u64 reach_arena_hint = 0;     // arena entries the last reachability evaluation used
     bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
@@ -2210,7 +2210,8 @@ bool run_scc_dense(ra_program* p, Scc& s)
 // Device buffers of one reachability evaluation, freed on every exit.
 struct ReachBufs {
     ra_program* p;
-    u32 *sval = nullptr, *indeg = nullptr, *rpar = nullptr, *rem = nullptr, *queue = nullptr, *seg_len = nullptr;
+    u32 *sval = nullptr, *indeg = nullptr, *rpar = nullptr, *rem = nullptr, *seg_len = nullptr;
+    u32 *front0 = nullptr, *front1 = nullptr, *hlist = nullptr;
     u32* flags = nullptr;
     u64 *rcsr = nullptr, *ctr = nullptr, *seg_off = nullptr, *row_new = nullptr, *row_off = nullptr;
     u64 *level_total = nullptr, *arena = nullptr;
@@ -2221,7 +2222,8 @@ struct ReachBufs {
     explicit ReachBufs(ra_program* pp) : p(pp) {}
     ~ReachBufs()
     {
-        for (u32** q : {&sval, &indeg, &rpar, &rem, &queue, &seg_len, &flags, &cyc, &c_node, &c_xnode, &c_xdist})
+        for (u32** q : {&sval, &indeg, &rpar, &rem, &front0, &front1, &hlist, &seg_len, &flags, &cyc, &c_node,
+                        &c_xnode, &c_xdist})
             dev_free(p, q);
         for (u64** q : {&rcsr, &ctr, &seg_off, &row_new, &row_off, &level_total, &arena, &cyc_n, &c_soff, &c_singles,
                         &c_xoff})
@@ -2230,6 +2232,15 @@ struct ReachBufs {
 };
 
 constexpr u64 kReachLevels = 1ull << kDistBits;   // distances fit 16 bits
+
+// A failed index check of the reachability kernels (none was dereferenced).
+void reach_check_corrupt(ra_program* p, u32 fl, const std::vector<u64>& hc)
+{
+    if (fl & kReachCorrupt)
+        fail(p, RA_E_CUDA, "reachability evaluator: index check %llu failed (value %llu, bound %llu)",
+             (unsigned long long)(hc[kCCheck] - 1), (unsigned long long)hc[kCCheck + 1],
+             (unsigned long long)hc[kCCheck + 2]);
+}
 
 // Runs SCC s with the reachability evaluator (ra_reach.cuh) when its one rule has
 // the transitive-closure shape and R's stored tuples are exactly S reversed;
@@ -2259,16 +2270,19 @@ bool run_scc_reach(ra_program* p, Scc& s)
     if (n > 16 * sn + (1u << 16)) return false;   // a sparse value domain: per-value arrays would dwarf the input
     const u64* scsr = version_csr(p, S, RA_FULL);
 
+    const auto t_setup = std::chrono::steady_clock::now();
     ReachBufs B(p);
     dev_alloc(p, &B.sval, sn);
     dev_alloc(p, &B.indeg, n + 1);
     dev_alloc(p, &B.rcsr, n + 1);
     dev_alloc(p, &B.rpar, sn);
     dev_alloc(p, &B.rem, n);
-    dev_alloc(p, &B.queue, n);
+    dev_alloc(p, &B.front0, n);
+    dev_alloc(p, &B.front1, n);
+    dev_alloc(p, &B.hlist, n);
     dev_alloc(p, &B.seg_len, n);
     dev_alloc(p, &B.seg_off, n);
-    dev_alloc(p, &B.ctr, 8);
+    dev_alloc(p, &B.ctr, kCtrWords);
     dev_alloc(p, &B.flags, 1);
     // predecessor lists (a counting sort of S by column 1)
     CK(cudaMemsetAsync(B.indeg, 0, (n + 1) * 4, p->stream));
@@ -2285,7 +2299,6 @@ bool run_scc_reach(ra_program* p, Scc& s)
     a.rcsr = B.rcsr;
     a.rpar = B.rpar;
     a.rem = B.rem;
-    a.queue = B.queue;
     a.ctr = B.ctr;
     a.seg_off = B.seg_off;
     a.seg_len = B.seg_len;
@@ -2304,41 +2317,48 @@ bool run_scc_reach(ra_program* p, Scc& s)
         int dev = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reach_dataflow_kernel, kThreads, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reach_levels_kernel, kThreads, 0));
         if (occ < 1) fail(p, RA_E_CUDA, "the reachability kernel does not fit on an SM");
     }
-    const auto t0 = std::chrono::steady_clock::now();
+    auto tp = t_setup;
+    auto phase_done = [&](int k) {   // host time since the last mark, after a synchronisation
+        const auto now = std::chrono::steady_clock::now();
+        p->stats.reach_phase_ms[k] += std::chrono::duration<double, std::milli>(now - tp).count();
+        tp = now;
+    };
+    phase_done(0);
     u64 cap = std::max<u64>(p->reach_arena_hint, 24 * sn + (1u << 20));
-    std::vector<u64> hc(8);
+    std::vector<u64> hc(kCtrWords);
     for (;;) {
         dev_free(p, &B.arena);
         dev_alloc(p, &B.arena, cap);
         a.arena = B.arena;
         a.arena_cap = cap;
-        CK(cudaMemsetAsync(B.ctr, 0, 8 * 8, p->stream));
+        CK(cudaMemsetAsync(B.ctr, 0, kCtrWords * 8, p->stream));
         CK(cudaMemsetAsync(B.flags, 0, 4, p->stream));
-        reach_init_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a);
+        reach_init_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a, B.front0);
         LAUNCHED();
-        reach_sinks_kernel<<<grid_for(n), kThreads, 0, p->stream>>>(a);
-        LAUNCHED();
-        void* args[] = {&a};
-        CK(cudaLaunchCooperativeKernel((const void*)reach_dataflow_kernel, dim3(sms * occ), dim3(kThreads), args, 0,
+        void* args[] = {&a, &B.front0, &B.front1, &B.hlist};
+        CK(cudaLaunchCooperativeKernel((const void*)reach_levels_kernel, dim3(sms * occ), dim3(kThreads), args, 0,
                                        p->stream));
         LAUNCHED();
         CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
-        CK(cudaMemcpyAsync(hc.data(), B.ctr, 8 * 8, cudaMemcpyDeviceToHost, p->stream));
+        CK(cudaMemcpyAsync(hc.data(), B.ctr, kCtrWords * 8, cudaMemcpyDeviceToHost, p->stream));
         CK(cudaStreamSynchronize(p->stream));
+        reach_check_corrupt(p, fl, hc);
         if (fl & kReachTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a bounded wait of the reachability evaluator gave up", s.id);
         if (fl & kReachArena) {   // room for what it asked, and some
-            cap = std::max<u64>(2 * cap, hc[3] + hc[3] / 4);
+            cap = std::max<u64>(2 * cap, hc[kCArena] + hc[kCArena] / 4);
             p->stats.regrows++;
             continue;
         }
         break;
     }
+    phase_done(1);
     if (fl & kReachDepth) return false;
     // nodes that reach a cycle: searched on the host over that part of the graph
-    const u64 finished = hc[2];
+    const u64 finished = hc[kCDone];
+    p->stats.reach_levels += hc[kCLevels];
     if (finished < n) {
         const u64 U = n - finished;
         if (U > std::max<u64>(1u << 16, n / 64)) return false;   // mostly cyclic: the semi-naive loop
@@ -2354,7 +2374,7 @@ bool run_scc_reach(ra_program* p, Scc& s)
         // successors of those nodes (S's rows are the CSR ranges), gathered on the device
         CK(cudaMemcpyAsync(B.cyc, cyc.data(), U * 4, cudaMemcpyHostToDevice, p->stream));
         dev_alloc(p, &B.c_soff, 2 * U);
-        reach_gather_ranges_kernel<<<grid_for(U), kThreads, 0, p->stream>>>(scsr, B.cyc, U, B.c_soff);
+        reach_gather_ranges_kernel<<<grid_for(U), kThreads, 0, p->stream>>>(scsr, B.cyc, U, n, B.c_soff);
         LAUNCHED();
         std::vector<u64> lohi(2 * U), off(U + 1);
         CK(cudaMemcpyAsync(lohi.data(), B.c_soff, 2 * U * 8, cudaMemcpyDeviceToHost, p->stream));
@@ -2446,12 +2466,13 @@ bool run_scc_reach(ra_program* p, Scc& s)
                                   p->stream>>>(a, c);
             LAUNCHED();
             CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
-            CK(cudaMemcpyAsync(hc.data(), B.ctr, 8 * 8, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaMemcpyAsync(hc.data(), B.ctr, kCtrWords * 8, cudaMemcpyDeviceToHost, p->stream));
             CK(cudaStreamSynchronize(p->stream));
+            reach_check_corrupt(p, fl, hc);
             if (fl & kReachDepth) return false;
             if (!(fl & kReachArena)) break;
             // a larger arena, keeping what the cycle-free nodes wrote
-            const u64 ncap = std::max<u64>(2 * cap, hc[3] + hc[3] / 4);
+            const u64 ncap = std::max<u64>(2 * cap, hc[kCArena] + hc[kCArena] / 4);
             u64* na;
             dev_alloc(p, &na, ncap);
             CK(cudaMemcpyAsync(na, B.arena, cap * 8, cudaMemcpyDeviceToDevice, p->stream));
@@ -2461,10 +2482,11 @@ bool run_scc_reach(ra_program* p, Scc& s)
             a.arena_cap = cap = ncap;
             p->stats.regrows++;
             // the failed launch's allocations are past the old end: nothing it wrote is kept
-            CK(cudaMemcpyAsync(B.ctr + 3, &hc[3], 8, cudaMemcpyHostToDevice, p->stream));
+            CK(cudaMemcpyAsync(B.ctr + kCArena, &hc[kCArena], 8, cudaMemcpyHostToDevice, p->stream));
         }
     }
-    p->reach_arena_hint = std::max<u64>(p->reach_arena_hint, hc[3] + hc[3] / 8);
+    p->reach_arena_hint = std::max<u64>(p->reach_arena_hint, hc[kCArena] + hc[kCArena] / 8);
+    phase_done(2);
 
     // new tuples, row by row, after R's stored ones
     dev_alloc(p, &B.row_new, n);
@@ -2478,12 +2500,17 @@ bool run_scc_reach(ra_program* p, Scc& s)
     CK(cudaMemsetAsync(B.level_total, 0, (kReachLevels + 1) * 8, p->stream));
     reach_emit_kernel<<<std::min<u64>((n + kWarps - 1) / kWarps, (u64)kSms * 16), kThreads, 0, p->stream>>>(
         a, B.row_off, p->bits, R.keys + n_stored, R.ids + n_stored, (u64)R.tag << 46, intern_counter(p, R.tag),
-        B.level_total, kReachLevels, B.level_total + kReachLevels);
+        B.level_total, kReachLevels, B.level_total + kReachLevels, total);
     LAUNCHED();
     std::vector<u64> lv(kReachLevels + 1);
     CK(cudaMemcpyAsync(lv.data(), B.level_total, (kReachLevels + 1) * 8, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(&fl, B.flags, 4, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(hc.data(), B.ctr, kCtrWords * 8, cudaMemcpyDeviceToHost, p->stream));
     CK(cudaStreamSynchronize(p->stream));
-    p->stats.reach_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    reach_check_corrupt(p, fl, hc);
+    phase_done(3);
+    p->stats.reach_ms = p->stats.reach_phase_ms[0] + p->stats.reach_phase_ms[1] + p->stats.reach_phase_ms[2] +
+                         p->stats.reach_phase_ms[3];
     u64 L = 0;
     while (L < kReachLevels && lv[L]) L++;
     p->stats.join_candidates += lv[kReachLevels];   // what the semi-naive loop's joins would have produced
@@ -2836,7 +2863,7 @@ int ra_program_create(int device, ra_program** out)
         CK(cudaMallocHost(&p->hctl, sizeof(IterCtl)));
         if (const char* e = getenv("RA_NO_GRAPH")) p->use_graphs = atoi(e) == 0;
         if (const char* e = getenv("RA_PERSIST")) p->use_persist = atoi(e) != 0;
-        if (const char* e = getenv("RA_NO_REACH")) p->use_reach = atoi(e) == 0;
+        if (const char* e = getenv("RA_REACH")) p->use_reach = atoi(e) != 0;
         if (const char* e = getenv("RA_KERNEL_EVENTS")) p->kernel_events = atoi(e) != 0;
     });
     if (st != RA_OK) {
@@ -2948,6 +2975,15 @@ int ra_program_set_launch_timing(ra_program* p, int on)
     return guard(p, [&] {
         if (p->running) fail(p, RA_E_STATE, "launch timing cannot change during a run");
         p->kernel_events = on != 0;
+    });
+}
+
+int ra_program_set_evaluators(ra_program* p, int reach, int persistent)
+{
+    return guard(p, [&] {
+        if (p->running) fail(p, RA_E_STATE, "evaluators cannot change during a run");
+        p->use_reach = reach != 0;
+        p->use_persist = persistent != 0;
     });
 }
 

@@ -28,7 +28,7 @@ E_BADARG, E_IO, E_OOM, E_CUDA, E_UNSUPPORTED, E_TIMEOUT, E_STATE = 1, 2, 3, 4, 5
 # every entry point declared in include/ra_engine.h
 EXPORTS = (
     "ra_program_create", "ra_program_destroy", "ra_program_set_stream", "ra_program_set_batch_size",
-    "ra_program_set_id_order", "ra_program_set_launch_timing",
+    "ra_program_set_id_order", "ra_program_set_launch_timing", "ra_program_set_evaluators",
     "ra_relation_create", "ra_relation_load_rows", "ra_relation_load_rows_device", "ra_relation_load_file",
     "ra_scc_create", "ra_scc_add_relation", "ra_scc_add_join", "ra_scc_add_copy", "ra_scc_depend",
     "ra_program_execute", "ra_program_run_next_scc", "ra_program_reset", "ra_program_history", "ra_program_stats", "ra_program_iteration_times",
@@ -55,7 +55,8 @@ class Stats(C.Structure):
         ("graph_build_ms", C.c_double), ("regrows", C.c_uint64), ("device_bytes", C.c_uint64),
         ("device_bytes_peak", C.c_uint64), ("dense_sccs", C.c_uint64), ("dense_search_ms", C.c_double),
         ("dense_emit_ms", C.c_double), ("bitmap_relations", C.c_uint64),
-        ("persistent_launches", C.c_uint64), ("reach_sccs", C.c_uint64), ("reach_ms", C.c_double),
+        ("persistent_launches", C.c_uint64), ("reach_sccs", C.c_uint64), ("reach_levels", C.c_uint64),
+        ("reach_ms", C.c_double), ("reach_phase_ms", C.c_double * 4),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 
@@ -92,6 +93,7 @@ def lib():
         L.ra_program_set_batch_size.argtypes = [P, C.c_uint32]
         L.ra_program_set_id_order.argtypes = [P, C.c_int]
         L.ra_program_set_launch_timing.argtypes = [P, C.c_int]
+        L.ra_program_set_evaluators.argtypes = [P, C.c_int, C.c_int]
         L.ra_relation_create.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int, i32p]
         L.ra_relation_load_rows.argtypes = [P, C.c_int, u64p, C.c_uint64]
         L.ra_relation_load_rows_device.argtypes = [P, C.c_int, C.c_void_p, C.c_uint64]
@@ -187,6 +189,12 @@ class Program:
     def set_launch_timing(self, on: bool):
         """Per-launch CUDA events on every iteration kernel (no CUDA graph while on)."""
         self._ck(self._L.ra_program_set_launch_timing(self._p, int(bool(on))), "set_launch_timing")
+
+    def set_evaluators(self, reach: bool = True, persistent: bool = False):
+        """reach: closure-shaped SCCs by composing reachable sets; persistent: other
+        device-driven SCCs as one cooperative launch (results are the same either way)."""
+        self._ck(self._L.ra_program_set_evaluators(self._p, int(bool(reach)), int(bool(persistent))),
+                 "set_evaluators")
 
     def set_batch_size(self, n: int):
         self._ck(self._L.ra_program_set_batch_size(self._p, n), "set_batch_size")

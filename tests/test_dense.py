@@ -12,9 +12,11 @@ pytestmark = pytest.mark.gpu
 
 
 def run(rows, dense, program="tc"):
+    """dense: the dense evaluator; otherwise the semi-naive hash-set path."""
     p = P.Program(0)
     if not dense:
         p.set_tuning(dense_max_bytes=0)
+        p.set_evaluators(reach=False)
     rels = P.programs.PROGRAMS[program](p, rows)
     p.execute(1)
     return p, rels
@@ -104,6 +106,7 @@ def test_bitmap_join_with_deltas_beyond_the_candidate_buffer():
     n = 16384
     rows = er(n, 2 * n, 12)
     pb = P.Program(0)
+    pb.set_evaluators(reach=False)
     pb.set_tuning(dense_max_bytes=8 * n * (n // 32) + 4 * n)
     rb = P.programs.build_tc(pb, rows)
     pb.execute(1)
