@@ -54,8 +54,14 @@ DESCRIBED = {"worstcase-110-terms-4-m": "0-CFA-style analysis of a generated 110
              "cfa-4-4-64": "k-CFA analysis (37 relations, arity <= 23, joins on 0..16 columns)"}
 OUTPUT = {"tc": "T", "sg": "SG"}
 INPUT = {"tc": "G", "sg": "edge"}
-# bounded CPU samples of the same graph families
+# bounded CPU samples of the same graph families (the cpu_baseline of our arm, and the
+# reference arm of workloads in REFERENCE_SAMPLED)
 CPU_SAMPLES = {"tc": ("er", (1 << 17, round(0.95 * (1 << 17)), 2)), "sg": ("tree", (1 << 12, 3))}
+# the reference's same generation on the 2^15-node tree holds ~4.6e8 tuples in its B-tree
+# tries: about 70 GB of host memory (1.51 GB measured for the 2^12-node tree's 9.8e6), more
+# than the box offers the arm; its reference arm runs the 2^12-node sample instead
+REFERENCE_SAMPLED = {"sg-tree15"}
+REFERENCE_ARM_SECONDS = 600.0
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
 # ncu capture in profiles/join_fused_kernel_tc-er20.md (1.86 / 1.87 / 1.87 over
@@ -150,7 +156,8 @@ def reference_rows_run(rows, kind="tc"):
             edge, empty, out = (os.path.join(tmp, x) for x in ("edge", "empty", "out"))
             P.datagen.write_relation(edge, rows)
             P.datagen.write_empty_relation(empty)
-            subprocess.run([drv, kind, edge, empty, out], check=True, stdout=subprocess.DEVNULL)
+            subprocess.run([drv, kind, edge, empty, out], check=True, stdout=subprocess.DEVNULL,
+                           env=dict(os.environ, RA_REF_NODUMP="1"))
             secs = float(open(os.path.join(out, "time.txt")).read())
             tc = next(int(l.split()[2]) for l in open(os.path.join(out, "sizes.txt"))
                       if l.split()[0] == OUTPUT[kind])
@@ -273,22 +280,37 @@ def run_reference_arm(args, rank, world):
                                                 "metric_family": METRIC_FAMILY},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "instances/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
-    prog_kind = WORKLOADS[args.workload][0]
+    prog_kind, gen, params = WORKLOADS[args.workload]
+    if args.workload in REFERENCE_SAMPLED:
+        # the reference needs more host memory than this workload's input allows (see REFERENCE_SAMPLED)
+        rows, desc, same = None, cpu_sample_desc(prog_kind), False
+    else:
+        rows = workload_rows(gen, params)
+        desc = (f"the workload's own input ({args.workload}: {gen} {list(params)}, {rows.shape[0]} rows), "
+                f"fixpoint time only")
+        same = True
+    # every step is a whole run of the reference (minutes at 2^22 nodes on one core): steps
+    # are taken while the arm's time stays within REFERENCE_ARM_SECONDS, at least one
     vals = []
-    for i in range(args.warmup + args.steps):
-        tc, secs, kind = reference_sample_run(prog_kind)
-        if i >= args.warmup:
-            vals.append((tc, secs))
+    t_start = time.time()
+    while len(vals) < args.steps:
+        tc, secs, kind = reference_rows_run(rows, prog_kind) if rows is not None else reference_sample_run(prog_kind)
+        vals.append((tc, secs))
+        if time.time() - t_start > REFERENCE_ARM_SECONDS * len(vals) / (len(vals) + 1):
+            break
     tot_tc = sum(v[0] for v in vals)
     tot_s = sum(v[1] for v in vals)
     value = tot_tc / tot_s
     line = {
         "impl": "reference", "metric": metric_of(prog_kind), "value": value, "unit": "tuples/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / len(vals), "higher_is_better": True,
+        "steps": len(vals), "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": 1e3 * tot_s / len(vals), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": cpu_sample_desc(prog_kind), "metric_family": METRIC_FAMILY},
-        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": 1, "kind": kind,
-                         "sample": cpu_sample_desc(prog_kind)},
+        "config": {"workload": args.workload, "sample": desc, "same_config": same, "output_tuples": vals[0][0],
+                   "steps_note": "each step is one whole run of the reference on one core; no warm-up (CPU "
+                                 "code, nothing to compile or cache across runs)",
+                   "metric_family": METRIC_FAMILY},
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": 1, "kind": kind, "sample": desc},
         "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -387,6 +409,28 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms, e2e_units = reduce_ranks(1e3 * statistics.mean(e2e_s), tc, f"cuda:{local_rank}")
     e2e = {"value": e2e_units / (e2e_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": int(rows.nbytes),
            "d2h_bytes_per_step": int(d2h)}
+    # the same, for a caller that wants the derived relation itself: its rows (data columns
+    # and intern ids, trie order) read back to host memory inside the timed region
+    e2e_rows_s = []
+    rows_d2h = 0
+    for i in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        prog.load_rows(in_rel, pinned_np)
+        for name, h_rel in rels.items():
+            if h_rel != in_rel:
+                prog.load_rows(h_rel, np.empty((0, 3), dtype=np.uint64))
+        prog.execute(1)
+        h = prog.history()
+        out_rows = prog.dump_full(out_rel)
+        e2e_rows_s.append(time.perf_counter() - t0)
+        rows_d2h = int(out_rows.nbytes) + 8 * (2 + sum(2 + 2 * len(x[1]) for x in h))
+        assert out_rows.shape[0] == tc
+        del out_rows
+    er_ms, er_units = reduce_ranks(1e3 * statistics.mean(e2e_rows_s), tc, f"cuda:{local_rank}")
+    e2e_rows = {"value": er_units / (er_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": int(rows.nbytes),
+                "d2h_bytes_per_step": rows_d2h,
+                "note": "e2e plus ra_relation_dump_full of the output relation (sorted rows with ids) to host"}
 
     peak, peak_kind = load_peaks()
     achieved = (dedup_bytes / dedup_launches) / ((dedup_ms / dedup_launches) / 1e3) / 1e9 if dedup_launches else 0.0
@@ -398,6 +442,17 @@ def run_ours(args, rank, world, local_rank):
                 "bytes_per_launch": dedup_bytes / max(dedup_launches, 1),
                 "bytes_model": "48 B per candidate (8 B inner key read, 8 B candidate write, 16 B seen-slot read "
                                "+ 16 B write) + 24 B per outer delta row (key, row offset, CSR start)"}
+    if not dense["sccs"] and dedup_launches and world == 1:
+        # the claims' own ceiling on this GPU: random 16-byte CAS on a table of the seen set's size
+        cal = P.engine.calibrate_random_access(local_rank, slots=max(1 << 20, int(tc / 0.45)), ops=64 << 20)
+        claims_per_s = st.join_candidates / (dedup_ms / max(1, min(args.steps, 3)) / 1e3) if dedup_ms else 0.0
+        roofline["random_access_ceiling"] = {
+            "cas16_per_s": cal["cas16_per_s"], "load8_per_s": cal["load8_per_s"], "table_bytes": cal["table_bytes"],
+            "claims_per_s": claims_per_s, "claims_frac_of_cas16": claims_per_s / cal["cas16_per_s"],
+            "note": "every candidate claims one 16-byte slot of a table far larger than L2; this GPU's rate "
+                    "of such random read-modify-writes, measured here, bounds the join kernel below the "
+                    "HBM copy roofline (linear probing adds ~1.3-2 CAS per candidate)"}
+
     if rank != 0:
         return None
     line = {
@@ -413,14 +468,60 @@ def run_ours(args, rank, world, local_rank):
                    "phase_ms_per_step": {k: v / max(1, min(args.steps, 3)) for k, v in
                                          zip(P.engine.Stats.PHASES, phase)},
                    "parallelism": f"{world} independent instance(s), one per GPU", "metric_family": METRIC_FAMILY},
-        "clocks": clocks.summary(), "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
-        "step_ms": step_ms,
+        "clocks": clocks.summary(), "e2e": e2e, "e2e_with_rows": e2e_rows, "gpu_launches": int(launches),
+        "roofline": roofline, "step_ms": step_ms,
     }
     if world == 1 and not args.no_cpu_baseline:
         ctc, csecs, kind = reference_sample_run(prog_kind)
         line["cpu_baseline"] = {"value": ctc / csecs, "unit": "tuples/s", "cores": 1, "kind": kind,
                                 "sample": cpu_sample_desc(prog_kind)}
+        golden = os.path.join(ROOT, "tests", "golden", GOLDEN_OF.get(args.workload, "") + ".json")
+        if args.workload in GOLDEN_OF and os.path.exists(golden):
+            g = json.load(open(golden))
+            if "reference_fixpoint_seconds_1core" in g:
+                line["cpu_baseline"]["same_input_reference_seconds"] = g["reference_fixpoint_seconds_1core"]
+                line["cpu_baseline"]["same_input_note"] = (
+                    "the reference's fixpoint time on this very input, one core, recorded when the golden "
+                    "vectors were generated (tests/golden/make_golden.py); `bench.py --impl reference` "
+                    "times it again on this box")
+    if world == 1 and args.workload == "tc-er22" and not args.no_extras:
+        # the other two patterns of the headline metric, bounded, in the same driver-run record
+        line["config"]["batched"] = batched_summary(args, local_rank)
+        line["config"]["served"] = served_summary(args, local_rank)
     return line
+
+
+# the golden record of each workload's own input (reference run), when one exists
+GOLDEN_OF = {"tc-er22": "er4194304_tc", "sg-tree15": "tree32768_sg", "tc-er2000": "er2000_tc"}
+
+
+def batched_summary(args, local_rank):
+    """The batched workload (8,192 TC instances against plain one-instance runs), one timed pass."""
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup = 1, 1
+    line = run_batched(sub, 0, 1, local_rank)
+    return {"instances": line["config"]["instances"], "instances_per_s": line["value"],
+            "e2e_instances_per_s": line["e2e"]["value"], "serial_instances_per_s": line["serial"]["value"],
+            "batched_over_serial": line["value"] / line["serial"]["value"],
+            "batched_e2e_over_serial": line["serial"]["batched_e2e_over_serial"],
+            "bit_exact_mismatches": line["serial"]["bit_exact_mismatches"], "waves": line["config"]["waves"],
+            "tuples_per_s": line["config"]["tuples_per_s"], "gpu_launches": line["gpu_launches"],
+            "step": "one timed pass over the batch (union rows resident), serial = plain runs of a random "
+                    f"sample of {BATCH_SERIAL_SAMPLE} instances from host rows, each checked bit-exact"}
+
+
+def served_summary(args, local_rank):
+    """The served workload at one arrival rate (the top of the sweep)."""
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup = 1, 1
+    line = run_served(sub, 0, 1, local_rank, rates=(max(SERVED_RATES),))
+    pt = line["config"]["rates"][0]
+    return {"rate_per_s": pt["rate"], "requests": line["config"]["requests"], "instances_per_s": line["value"],
+            "p50_ms": pt["p50_ms"], "p95_ms": pt["p95_ms"], "p99_ms": pt["p99_ms"],
+            "one_at_a_time_instances_per_s": line["one_at_a_time"]["value"],
+            "served_over_one_at_a_time": line["value"] / line["one_at_a_time"]["value"],
+            "bit_exact_checked": line["bit_exact"]["checked"], "bit_exact_mismatches": line["bit_exact"]["mismatches"],
+            "oom_retries": line["admission"]["oom_retries"], "waves": pt["waves"]}
 
 
 def described_paths(name):
@@ -727,11 +828,12 @@ def run_batched(args, rank, world, local_rank):
 
 SERVED_COUNT, SERVED_SEED = 20000, 4
 SERVED_RATES = (100.0, 1000.0, 10000.0)
+SERVED_RATES_DEFAULT = SERVED_RATES
 SERVED_POINT_SECONDS = 10.0
 SERVED_CHECK_SAMPLE = 400
 
 
-def run_served(args, rank, world, local_rank):
+def run_served(args, rank, world, local_rank, rates=SERVED_RATES_DEFAULT):
     """Open-loop Poisson request streams (80% TC, 20% SG, 2% large TC) against the
     continuous-batching server, swept over arrival rates; latency percentiles and
     instances/s per rate, every checked result equal to a plain single-instance run."""
@@ -750,12 +852,12 @@ def run_served(args, rank, world, local_rank):
 
     server = Server(local_rank, slots=args.slots, budget_bytes=args.budget_gb * 1e9)
     for _ in range(args.warmup):               # warm-up streams: graphs, buffers, learnt estimates
-        run_stream(server, clones(reqs[:500]), poisson_arrivals(500, max(SERVED_RATES), 99))
+        run_stream(server, clones(reqs[:500]), poisson_arrivals(500, max(rates), 99))
     points = []
     top = None
     with ClockSampler(local_rank) as clocks:
-        for rate in SERVED_RATES:
-            k = SERVED_COUNT if rate == max(SERVED_RATES) else min(SERVED_COUNT, int(rate * SERVED_POINT_SECONDS))
+        for rate in rates:
+            k = SERVED_COUNT if rate == max(rates) else min(SERVED_COUNT, int(rate * SERVED_POINT_SECONDS))
             stream = clones(reqs[:k])
             w0 = len(server.waves)
             if world > 1:
@@ -768,7 +870,7 @@ def run_served(args, rank, world, local_rank):
             st["gpu_launches"] = int(sum(w.launches for w in waves))
             st["max_held_gb"] = max(w.held_bytes for w in waves) / 1e9
             points.append(st)
-            if rate == max(SERVED_RATES):
+            if rate == max(rates):
                 top = (stream, st)
     server.close()
 
@@ -787,7 +889,7 @@ def run_served(args, rank, world, local_rank):
     # the same stream served one instance at a time (no batching, one worker)
     one = Server(local_rank, slots=1, budget_bytes=args.budget_gb * 1e9, max_wave_requests=1)
     k1 = 1500
-    st_one = run_stream(one, clones(reqs[:k1]), poisson_arrivals(k1, max(SERVED_RATES), 7))
+    st_one = run_stream(one, clones(reqs[:k1]), poisson_arrivals(k1, max(rates), 7))
     one.close()
     # whole job: every rank's top-rate stream over the slowest rank's serving time
     top_ms, served = reduce_ranks(1e3 * st_top["seconds"], len(stream), f"cuda:{local_rank}")
@@ -835,6 +937,8 @@ def main():
                     help="batched: estimated derived tuples per wave (default: the autotuned size, "
                          "capped by half the free device memory)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="tc-er22: leave out the bounded batched and served sub-records of config")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -175,6 +175,14 @@ int ra_program_set_memory_cap(ra_program* p, uint64_t bytes);
  * wait does instead of spinning forever; the context stays usable.  No
  * reference counterpart (the reference has no device waits). */
 int ra_selftest_bounded_wait(int device, uint64_t max_polls);
+/* Measures this GPU's random-access ceiling that bounds the seen-set claims of
+ * the semi-naive join: `ops` 16-byte compare-and-swaps, then `ops` 8-byte
+ * loads, at uniformly random slots of a fresh table of `slots` 16-byte slots
+ * (a claim's own access pattern, at the size of the workload's seen set).
+ * Writes the rates in operations per second to out_rates[0] (CAS) and
+ * out_rates[1] (loads).  Allocates and frees the table itself.  No reference
+ * counterpart (a measurement aid for the roofline of the claim kernels). */
+int ra_calibrate_random_access(int device, uint64_t slots, uint64_t ops, double* out_rates);
 /* Read / replace the program's tuning (RA_E_BADARG outside the ranges above;
  * RA_E_STATE during a run). */
 int ra_program_get_tuning(ra_program* p, ra_tuning* out);

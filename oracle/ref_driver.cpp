@@ -18,7 +18,8 @@
  *                   (a program description, its batch size from the file)
  * writes: <out_dir>/history.txt   "scc <id> <iters>" then "<sum_delta> <sum_full>" per batch
  *         <out_dir>/sizes.txt     "<name> <arity> <full_count>" per relation
- *         <out_dir>/<name>.bin    full relation rows (arity+1 u64, trie order = sorted)
+ *         <out_dir>/<name>.bin    full relation rows (arity+1 u64, trie order = sorted),
+ *                                 unless RA_REF_NODUMP=1 (timing runs)
  *         <out_dir>/time.txt      fixpoint seconds (sum over SCCs of execute_in_batches)
  */
 #include "parallel_RA_inc.h"
@@ -119,7 +120,7 @@ int main(int argc, char** argv)
     FILE* sz = fopen((out + "/sizes.txt").c_str(), "w");
     for (relation* r : p.relations) {
         fprintf(sz, "%s %u %d\n", r->get_debug_id().c_str(), r->get_arity(), r->get_full_element_count());
-        dump_relation(r, out + "/" + r->get_debug_id() + ".bin");
+        if (!getenv("RA_REF_NODUMP")) dump_relation(r, out + "/" + r->get_debug_id() + ".bin");
     }
     fclose(sz);
     FILE* tf = fopen((out + "/time.txt").c_str(), "w");

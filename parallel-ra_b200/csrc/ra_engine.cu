@@ -3235,6 +3235,68 @@ int ra_selftest_bounded_wait(int device, uint64_t max_polls)
     return st;
 }
 
+namespace {
+// kind 0: empty -> key CAS on 16-byte slots; kind 1: 8-byte loads.  Four independent
+// accesses per thread in flight, slots from the claims' own hash of the operation index.
+__global__ void __launch_bounds__(kThreads) calibrate_kernel(Slot* __restrict__ t, u64 cap, u64 ops, u64 salt, int kind,
+                                                             u64* __restrict__ sink)
+{
+    u64 acc = 0;
+    const u64 stride = (u64)gridDim.x * kThreads * 4;
+    for (u64 i0 = ((u64)blockIdx.x * kThreads + threadIdx.x) * 4; i0 < ops; i0 += stride) {
+        u64 h[4];
+#pragma unroll
+        for (int b = 0; b < 4; b++) h[b] = slot_start(i0 + b + salt, cap);
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            if (i0 + b >= ops) continue;
+            if (kind == 0) {
+                const Slot r = atomicCAS(&t[h[b]], Slot{kEmpty, ~0ull}, Slot{i0 + b, salt});
+                acc += r.key;
+            } else {
+                acc += __ldcg(&t[h[b]].key);
+            }
+        }
+    }
+    if (acc == 0x5eed) *sink = acc;   // keeps the accesses
+}
+}  // namespace
+
+int ra_calibrate_random_access(int device, uint64_t slots, uint64_t ops, double* out_rates)
+{
+    if (!out_rates || slots < 1024 || ops == 0) return RA_E_BADARG;
+    if (cudaSetDevice(device) != cudaSuccess) return RA_E_CUDA;
+    Slot* t = nullptr;
+    u64* sink = nullptr;
+    if (cudaMalloc(&t, slots * sizeof(Slot)) != cudaSuccess) return RA_E_OOM;
+    if (cudaMalloc(&sink, 8) != cudaSuccess) {
+        cudaFree(t);
+        return RA_E_OOM;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int st = RA_OK;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = RA_E_CUDA;
+    for (int kind = 0; kind < 2 && st == RA_OK; kind++) {
+        float best = 0;
+        for (int rep = 0; rep < 3 && st == RA_OK; rep++) {
+            if (cudaMemset(t, 0xff, slots * sizeof(Slot)) != cudaSuccess) st = RA_E_CUDA;
+            cudaEventRecord(e0);
+            calibrate_kernel<<<kSms * 8, kThreads>>>(t, slots, ops, 1000003ull * (rep + 1), kind, sink);
+            cudaEventRecord(e1);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) st = RA_E_CUDA;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep == 0 || ms < best) best = ms;
+        }
+        out_rates[kind] = best > 0 ? (double)ops / (best / 1e3) : 0.0;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(sink);
+    cudaFree(t);
+    return st;
+}
+
 int ra_program_set_checkpoint(ra_program* p, const char* output_dir, uint32_t every_batches, int separate_files)
 {
     return guard(p, [&] {

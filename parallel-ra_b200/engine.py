@@ -36,7 +36,7 @@ EXPORTS = (
     "ra_program_set_instances", "ra_program_instance_history", "ra_relation_instance_summary",
     "ra_program_get_tuning", "ra_program_set_tuning", "ra_program_release",
     "ra_program_set_checkpoint", "ra_program_set_restart", "ra_program_set_memory_cap",
-    "ra_selftest_bounded_wait",
+    "ra_selftest_bounded_wait", "ra_calibrate_random_access",
 )
 
 
@@ -111,6 +111,7 @@ def lib():
         L.ra_program_set_restart.argtypes = [P, C.c_char_p, C.c_int]
         L.ra_program_set_memory_cap.argtypes = [P, C.c_uint64]
         L.ra_selftest_bounded_wait.argtypes = [C.c_int, C.c_uint64]
+        L.ra_calibrate_random_access.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_double)]
         L.ra_program_history.argtypes = [P, u64p, C.c_uint64, u64p]
         L.ra_program_stats.argtypes = [P, C.POINTER(Stats)]
         L.ra_program_iteration_times.argtypes = [P, C.POINTER(C.c_double), C.c_uint64, u64p]
@@ -348,3 +349,14 @@ class Program:
 def selftest_bounded_wait(device: int = 0, max_polls: int = 1 << 16) -> int:
     """Status of the engine's bounded-wait self-test (E_TIMEOUT when the wait gave up as designed)."""
     return lib().ra_selftest_bounded_wait(device, max_polls)
+
+
+def calibrate_random_access(device: int = 0, slots: int = 177 << 20, ops: int = 64 << 20) -> dict:
+    """This GPU's random 16-byte CAS and 8-byte load rates (operations/s) on a table
+    of `slots` 16-byte slots: the ceiling of the seen-set claims."""
+    out = (C.c_double * 2)()
+    st = lib().ra_calibrate_random_access(device, slots, ops, out)
+    if st != 0:
+        raise RAError(st, f"ra_calibrate_random_access: {lib().ra_status_string(st).decode()}")
+    return {"cas16_per_s": out[0], "load8_per_s": out[1], "table_bytes": 16 * slots}
+
