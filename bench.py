@@ -215,6 +215,8 @@ def reduce_ranks(total_ms, count, device):
     import torch.distributed as dist
     if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
         return float(total_ms), int(count)
+    if dist.get_backend() == "gloo":
+        device = "cpu"
     t = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     c = torch.tensor([float(count)], dtype=torch.float64, device=device)
@@ -320,16 +322,30 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import parallel_ra_b200 as P
 
-    torch.cuda.set_device(local_rank)
+    dev = local_rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
     prog_kind, gen, params = WORKLOADS[args.workload]
-    params = params[:-1] + (params[-1] + 1000 * rank,)     # each rank: its own independent instance
+    partitioned = world > 1 and prog_kind == "tc" and gen == "er"
+    if partitioned:
+        # one instance N times the size, T partitioned over the ranks by source (partition.py):
+        # every rank generates the same graph, keeps G whole and seeds T with the edges it owns
+        n, m, seed = params
+        params = (n * world, m * world, seed)
+    else:
+        params = params[:-1] + (params[-1] + 1000 * rank,)     # each rank: its own independent instance
     rows = workload_rows(gen, params)
     stream = torch.cuda.Stream()
-    prog = P.Program(local_rank)
+    prog = P.Program(dev)
     prog.set_stream(stream.cuda_stream)
-    rels = P.programs.PROGRAMS[prog_kind](prog, rows)
-    out_rel, in_rel = rels[OUTPUT[prog_kind]], rels[INPUT[prog_kind]]
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f"cuda:{local_rank}")
+    if partitioned:
+        rels = P.partition.build_tc_partitioned(prog, rows, rank, world)
+        own = P.partition.owner(rows[:, 0], world) == rank
+        inputs = {"G": rows, "G_own": np.ascontiguousarray(rows[own]), "T": np.empty((0, 3), dtype=np.uint64)}
+    else:
+        rels = P.programs.PROGRAMS[prog_kind](prog, rows)
+        inputs = {name: (rows if name == INPUT[prog_kind] else np.empty((0, 3), dtype=np.uint64)) for name in rels}
+    out_rel = rels[OUTPUT[prog_kind]]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f"cuda:{dev}")
 
     for _ in range(args.warmup):
         prog.execute(1)
@@ -359,9 +375,14 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms, tc_all = reduce_ranks(sum(step_ms), tc, f"cuda:{local_rank}")
+    total_ms, tc_all = reduce_ranks(sum(step_ms), tc, f"cuda:{dev}")
     value = tc_all * args.steps / (total_ms / 1e3)
     st = prog.stats()
+    iterations = int(st.iterations)
+    if partitioned:
+        # the single-instance history from every rank's (one exchange, after the timing)
+        gh = P.partition.global_history(prog.history())
+        iterations = sum(len(h) for _, h in gh)
 
     # dominant kernel (fused join count, scan, expansion + first-occurrence claim): per-launch
     # CUDA events on the engine's stream, in an instrumented pass over the same
@@ -389,25 +410,28 @@ def run_ours(args, rank, world, local_rank):
     prog.set_id_order(P.engine.IDS_EMISSION)
 
     # end to end through the C ABI from pinned host rows
-    pinned = torch.from_numpy(rows.view(np.int64)).pin_memory()
-    pinned_np = pinned.numpy().view(np.uint64)
+    pinned_in = {name: torch.from_numpy(np.ascontiguousarray(r).view(np.int64)).pin_memory().numpy().view(np.uint64)
+                 for name, r in inputs.items()}
+    h2d_bytes = int(sum(r.nbytes for r in inputs.values()))
+
+    def load_inputs():
+        for name, r in pinned_in.items():
+            prog.load_rows(rels[name], r)
+
     e2e_s = []
     d2h = 0
     for i in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        prog.load_rows(in_rel, pinned_np)
-        for name, h_rel in rels.items():
-            if h_rel != in_rel:
-                prog.load_rows(h_rel, np.empty((0, 3), dtype=np.uint64))
+        load_inputs()
         prog.execute(1)
         h = prog.history()
         f, _ = prog.counts(out_rel)
         e2e_s.append(time.perf_counter() - t0)
         d2h = 8 * (2 + sum(2 + 2 * len(x[1]) for x in h))
         assert f == tc
-    e2e_ms, e2e_units = reduce_ranks(1e3 * statistics.mean(e2e_s), tc, f"cuda:{local_rank}")
-    e2e = {"value": e2e_units / (e2e_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": int(rows.nbytes),
+    e2e_ms, e2e_units = reduce_ranks(1e3 * statistics.mean(e2e_s), tc, f"cuda:{dev}")
+    e2e = {"value": e2e_units / (e2e_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": h2d_bytes,
            "d2h_bytes_per_step": int(d2h)}
     # the same, for a caller that wants the derived relation itself: its rows (data columns
     # and intern ids, trie order) read back to host memory inside the timed region
@@ -416,10 +440,7 @@ def run_ours(args, rank, world, local_rank):
     for i in range(max(1, min(args.steps, 2))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        prog.load_rows(in_rel, pinned_np)
-        for name, h_rel in rels.items():
-            if h_rel != in_rel:
-                prog.load_rows(h_rel, np.empty((0, 3), dtype=np.uint64))
+        load_inputs()
         prog.execute(1)
         h = prog.history()
         out_rows = prog.dump_full(out_rel)
@@ -427,8 +448,8 @@ def run_ours(args, rank, world, local_rank):
         rows_d2h = int(out_rows.nbytes) + 8 * (2 + sum(2 + 2 * len(x[1]) for x in h))
         assert out_rows.shape[0] == tc
         del out_rows
-    er_ms, er_units = reduce_ranks(1e3 * statistics.mean(e2e_rows_s), tc, f"cuda:{local_rank}")
-    e2e_rows = {"value": er_units / (er_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": int(rows.nbytes),
+    er_ms, er_units = reduce_ranks(1e3 * statistics.mean(e2e_rows_s), tc, f"cuda:{dev}")
+    e2e_rows = {"value": er_units / (er_ms / 1e3), "unit": "tuples/s", "h2d_bytes_per_step": h2d_bytes,
                 "d2h_bytes_per_step": rows_d2h,
                 "note": "e2e plus ra_relation_dump_full of the output relation (sorted rows with ids) to host"}
 
@@ -444,7 +465,7 @@ def run_ours(args, rank, world, local_rank):
                                "+ 16 B write) + 24 B per outer delta row (key, row offset, CSR start)"}
     if not dense["sccs"] and dedup_launches and world == 1:
         # the claims' own ceiling on this GPU: random 16-byte CAS on a table of the seen set's size
-        cal = P.engine.calibrate_random_access(local_rank, slots=max(1 << 20, int(tc / 0.45)), ops=64 << 20)
+        cal = P.engine.calibrate_random_access(dev, slots=max(1 << 20, int(tc / 0.45)), ops=64 << 20)
         claims_per_s = st.join_candidates / (dedup_ms / max(1, min(args.steps, 3)) / 1e3) if dedup_ms else 0.0
         roofline["random_access_ceiling"] = {
             "cas16_per_s": cal["cas16_per_s"], "load8_per_s": cal["load8_per_s"], "table_bytes": cal["table_bytes"],
@@ -460,14 +481,17 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": args.workload, "program": prog_kind, "generator": gen, "generator_args": list(params),
-                   "input_rows": int(rows.shape[0]), "output_tuples": tc, "iterations": int(st.iterations),
+                   "input_rows": int(rows.shape[0]), "output_tuples": tc_all, "iterations": iterations,
                    "join_candidates": int(st.join_candidates),
                    "value_bits": int(st.value_bits), "l2": "flushed (256 MiB write) before every timed step",
                    "id_order": "emission (default)",
                    "value_reference_ids": tc / (statistics.median(ref_ms) / 1e3),
                    "phase_ms_per_step": {k: v / max(1, min(args.steps, 3)) for k, v in
                                          zip(P.engine.Stats.PHASES, phase)},
-                   "parallelism": f"{world} independent instance(s), one per GPU", "metric_family": METRIC_FAMILY},
+                   "parallelism": (f"one instance of {world}x the size, T partitioned over {world} ranks by a hash of "
+                                   f"its source column, G replicated; no exchange (partition.py)" if partitioned else
+                                   f"{world} independent instance(s), one per GPU"),
+                   "metric_family": METRIC_FAMILY},
         "clocks": clocks.summary(), "e2e": e2e, "e2e_with_rows": e2e_rows, "gpu_launches": int(launches),
         "roofline": roofline, "step_ms": step_ms,
     }
@@ -950,8 +974,10 @@ def main():
         import torch
         import torch.distributed as dist
         if args.impl == "ours":
-            torch.cuda.set_device(local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            torch.cuda.set_device(local_rank % max(1, torch.cuda.device_count()))
+            # the ranks exchange only host-side scalars and histories: NCCL by default, or
+            # RA_BENCH_BACKEND=gloo (e.g. several ranks sharing one GPU in a smoke run)
+            dist.init_process_group(os.environ.get("RA_BENCH_BACKEND", "nccl"), timeout=datetime.timedelta(seconds=300))
     if args.impl == "reference":
         line = run_reference_arm(args, rank, world)
     elif args.workload in ("batched", "served"):

@@ -5,10 +5,10 @@ The engine is native: CUDA kernels for sm_100a plus a C ABI
 (relation, RAM, parallel_join, parallel_copy, parallel_copy_filter, LIE) in
 ``libparallel_ra.so``.  This Python package is a ctypes binding of the C ABI
 (``engine``), the TC / SG program definitions (``programs``), seeded input
-generators (``datagen``) and batched execution of many instances per launch
-(``batch``).
+generators (``datagen``), batched execution of many instances per launch
+(``batch``) and transitive closure partitioned over ranks (``partition``).
 """
-from . import batch, datagen, engine, programs  # noqa: F401
+from . import batch, datagen, engine, partition, programs  # noqa: F401
 from .engine import Program, RAError  # noqa: F401
 
-__all__ = ["Program", "RAError", "batch", "datagen", "engine", "programs"]
+__all__ = ["Program", "RAError", "batch", "datagen", "engine", "partition", "programs"]
