@@ -112,6 +112,9 @@ typedef struct ra_stats {
     double reach_ms;            /* host wall time of those evaluations (synchronised, launches included) */
     double reach_phase_ms[4];   /* of which: [0] graph set-up and checks, [1] the level sweep,
                                    [2] nodes that reach a cycle, [3] emission of the new tuples */
+    uint64_t sliced_iterations; /* iterations run in slices of outer rows: their candidates did not fit
+                                   the candidate buffer the memory cap (ra_program_set_memory_cap) allows */
+    uint64_t sliced_passes;     /* join + select passes of those iterations */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose

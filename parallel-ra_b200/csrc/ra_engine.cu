@@ -1037,6 +1037,7 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
     if (cand_cap > p->dcand_cap) {
         dev_free(p, &p->dcand);
         dev_free(p, &p->dloser);
+        p->dcand_cap = 0;   // a failed allocation leaves no capacity behind a freed buffer
         dev_alloc(p, &p->dcand, cand_cap);
         dev_alloc(p, &p->dloser, cand_cap);
         CK(cudaMemsetAsync(p->dloser, 0, cand_cap * 4, p->stream));   // epoch 0: no marks
@@ -1075,6 +1076,7 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
                                  max_outer / kPJChunk + 2, p->dcand_cap / kPSChunk + 2});
     if (st_need > p->status_cap) {
         dev_free(p, &p->status);
+        p->status_cap = 0;
         dev_alloc(p, &p->status, st_need);
         p->status_cap = st_need;
     }
@@ -1162,7 +1164,7 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
             join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
                                                              p->bits, p->dcand, p->dcand_cap, out.seen,
                                                              out.seen_cap, p->dloser, p->status, p->status_cap,
-                                                             slot++, d.bit[r.out_slot]);
+                                                             slot++, d.bit[r.out_slot], JoinSlice{0, 0, 0, 0});
         else
             copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
                                                                  p->dcand, p->dcand_cap, out.seen, out.seen_cap,
@@ -1590,6 +1592,121 @@ void ctl_download(ra_program* p)
     CK(cudaStreamSynchronize(p->stream));
 }
 
+// Can the running iteration of SCC s run in slices of outer rows?  Join rules
+// only, into hash seen sets, with new tuples written straight to the log.
+bool sliceable(ra_program* p, const DevScc& d)
+{
+    if (p->id_order != RA_IDS_EMISSION || p->n_inst) return false;
+    for (const DevRule& r : d.rules)
+        if (r.kind != kJoin || d.bit[r.out_slot].seen) return false;
+    return true;
+}
+
+// One iteration of SCC s in slices of outer rows, when its candidates exceed the
+// candidate buffer that the program's memory cap leaves room for (the
+// reference bounds a join call's output in the same spirit and resumes from an
+// offset, src/RAM/RA_tasks.cpp:312 and src/RA/parallel_join.cpp:196-201).  Per
+// rule, per slice of whole tiles: the join claims with the slice's stream
+// positions (so first occurrences and losers are the unsliced ones: a later
+// slice never displaces an earlier one's tuple) and its select appends the
+// slice's winners after the previous slices'.  Then the iteration end, as the
+// loop's.  The log, ids included, and the history are those of an unsliced
+// iteration.  Expects the control block downloaded in hctl.
+void run_sliced_iteration(ra_program* p, Scc& s, DevScc& d)
+{
+    IterCtl& h = *p->hctl;
+    // a sliced iteration appends as it goes and cannot be replayed: room for its history entry first
+    if (h.hist_n + 1 >= p->dhist_cap) {
+        dev_size_buffers(p, d, p->dcand_cap, p->stage_cap, 2 * p->dhist_cap);
+        CK(cudaMemcpyAsync(&p->ctl->time_cap, &p->hctl->time_cap, 8, cudaMemcpyHostToDevice, p->stream));
+    }
+    const SccPlan& pl = d.plan;
+    const int G = grid_blocks(p->tune.join_blocks_per_sm);
+    const int GS = grid_blocks(p->tune.select_blocks_per_sm);
+    std::vector<u64> appended(pl.n_rels, 0), id_app(kMaxTagSlots, 0), cand_tot(pl.n_rules, 0), win_tot(pl.n_rules, 0);
+    u64 pos = 0;   // stream position of the next rule's first candidate
+    u64* tile_cnt = nullptr;
+    struct Free {
+        ra_program* p;
+        u64** q;
+        ~Free() { dev_free(p, q); }
+    } free_tiles{p, &tile_cnt};
+    for (int q = 0; q < pl.n_rules; q++) {
+        const DevRule& r = d.rules[q];
+        Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
+        const u64 n = r.in.slot >= 0 ? h.delta_n[r.in.slot] : r.in.static_n;
+        const u64 ntiles = (n + kJRows - 1) / kJRows;
+        std::vector<u64> cnt(ntiles);
+        if (ntiles) {
+            dev_free(p, &tile_cnt);
+            dev_alloc(p, &tile_cnt, ntiles);
+            join_tile_counts_kernel<<<(int)std::min<u64>(ntiles, (u64)kMaxGrid), kThreads, 0, p->stream>>>(
+                p->ctl, r.in, r.outer_shift, r.csr, tile_cnt);
+            LAUNCHED();
+            CK(cudaMemcpyAsync(cnt.data(), tile_cnt, ntiles * 8, cudaMemcpyDeviceToHost, p->stream));
+            CK(cudaStreamSynchronize(p->stream));
+        }
+        u64 rule_pos = 0;
+        for (u64 t = 0; t < ntiles || (t == 0 && ntiles == 0);) {
+            u64 t1 = t, c = 0;
+            while (t1 < ntiles && c + cnt[t1] <= p->dcand_cap) c += cnt[t1++];
+            if (t1 == t && ntiles)
+                fail(p, RA_E_OOM, "SCC %d: %llu outer rows have %llu candidates, more than the %llu the memory cap "
+                                  "leaves room for", s.id, (unsigned long long)kJRows, (unsigned long long)cnt[t],
+                     (unsigned long long)p->dcand_cap);
+            const u64 lo = t * kJRows, rows = std::min(n, t1 * kJRows) - lo;
+            // a fresh slice: no marks, no look-back statuses, tile counters at zero
+            CK(cudaMemsetAsync(p->dloser, 0, std::max<u64>(c, 1) * 4, p->stream));
+            CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+            CK(cudaMemsetAsync(p->ctl->tile_ctr, 0, sizeof(p->ctl->tile_ctr), p->stream));
+            join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
+                                                             p->bits, p->dcand, p->dcand_cap, out.seen, out.seen_cap,
+                                                             p->dloser, p->status, p->status_cap, 0, d.bit[r.out_slot],
+                                                             JoinSlice{lo, rows, pos + rule_pos, 1});
+            LAUNCHED();
+            SelectArgs a{};
+            a.rule = q;
+            a.last = 0;
+            a.to_log = 1;
+            a.dst_keys = out.keys;
+            a.dst_ids = out.ids;
+            a.sliced = 1;
+            a.appended = appended[r.out_slot];
+            a.id_appended = id_app[pl.rule_tag[q]];
+            select_kernel<<<GS, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, a, p->dcand, p->dloser, p->status, 1,
+                                                         p->dhist, 0, 0);
+            LAUNCHED();
+            ctl_download(p);
+            if (h.flags & kFlagTimeout) fail(p, RA_E_TIMEOUT, "SCC %d: a device-side look-back wait gave up", s.id);
+            if (h.flags)
+                fail(p, RA_E_OOM, "SCC %d: a sliced iteration ran out of room (flags %u) under the memory cap", s.id,
+                     h.flags);
+            const u64 w = h.win_n[q];
+            appended[r.out_slot] += w;
+            id_app[pl.rule_tag[q]] += w;
+            cand_tot[q] += h.cand_n[q];
+            win_tot[q] += w;
+            rule_pos += c;
+            p->stats.sliced_passes++;
+            if (ntiles == 0) break;
+            t = t1;
+        }
+        pos += cand_tot[q];
+    }
+    // the iteration end with the iteration's totals, as the loop's last select runs it
+    for (int q = 0; q < pl.n_rules; q++) {
+        h.cand_n[q] = cand_tot[q];
+        h.win_n[q] = win_tot[q];
+    }
+    for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
+    CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
+    iter_end_kernel<<<64, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, p->dhist, 0, 0);
+    LAUNCHED();
+    ctl_download(p);
+    p->stats.sliced_iterations++;
+}
+
 // Kernel parameters of the persistent SCC kernel (ra_persist.cuh) for the plan's
 // current buffers and capacities.
 PersistArgs persist_args(ra_program* p, const DevScc& d)
@@ -1691,8 +1808,18 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     CK(cudaMemsetAsync(&p->ctl->sort_hist[0][0][0], 0, sizeof(p->ctl->sort_hist), p->stream));
     u64 outer0 = 0;
     for (const DevRule& r : d.rules) outer0 = std::max(outer0, r.in.slot >= 0 ? p->rels[d.rel_of_slot[r.in.slot]].delta_n : r.in.static_n);
-    dev_size_buffers(p, d, std::max<u64>({p->dcand_cap, 1u << 22, 2 * outer0}),
-                     std::max<u64>({p->stage_cap, 1u << 22, 2 * outer0}), std::max<u64>(p->dhist_cap, 1u << 12));
+    for (u64 want = std::max<u64>({p->dcand_cap, 1u << 22, 2 * outer0});; want /= 2) {
+        try {
+            dev_size_buffers(p, d, want, std::max<u64>({p->stage_cap, 1u << 22, 2 * outer0}),
+                             std::max<u64>(p->dhist_cap, 1u << 12));
+            break;
+        } catch (ra_error& e) {
+            // under a memory cap a smaller candidate buffer will do: iterations that outgrow
+            // it run in slices of outer rows (run_sliced_iteration)
+            if (e.status != RA_E_OOM || !sliceable(p, d) || want <= (1u << 12)) throw;
+            p->err.clear();
+        }
+    }
     CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
     CK(cudaMemcpyAsync(&p->ctl->time_cap, &p->hctl->time_cap, 8, cudaMemcpyHostToDevice, p->stream));
     if (p->n_inst) {
@@ -1795,9 +1922,37 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 }
             }
             refresh_refs(p, d);
-            dev_size_buffers(p, d, replay ? std::max(p->dcand_cap, 2 * total) : p->dcand_cap,
-                             replay ? std::max(p->stage_cap, 2 * stage_need) : p->stage_cap,
-                             h.hist_n >= p->dhist_cap ? 2 * p->dhist_cap : p->dhist_cap);
+            const bool cand_short = replay && total > p->dcand_cap;
+            try {
+                dev_size_buffers(p, d, replay ? std::max(p->dcand_cap, 2 * total) : p->dcand_cap,
+                                 replay ? std::max(p->stage_cap, 2 * stage_need) : p->stage_cap,
+                                 h.hist_n >= p->dhist_cap ? 2 * p->dhist_cap : p->dhist_cap);
+            } catch (ra_error& e) {
+                // the memory cap leaves no room for the iteration's candidates: the largest
+                // candidate buffer that fits, and the iteration in slices of outer rows
+                if (e.status != RA_E_OOM || !cand_short || !sliceable(p, d)) throw;
+                u64 cap = std::max<u64>(total / 2, 1u << 16);
+                for (;;) {
+                    try {
+                        dev_size_buffers(p, d, cap, p->stage_cap, p->dhist_cap);
+                        break;
+                    } catch (ra_error& e2) {
+                        if (e2.status != RA_E_OOM || cap <= (1u << 12)) throw;
+                        cap /= 2;
+                    }
+                }
+                p->err.clear();
+                h.flags = 0;
+                h.exit_ctr = 0;
+                h.bar_count = 0;
+                for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
+                CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
+                run_sliced_iteration(p, s, d);
+                if (h.flags & kFlagGrow) continue;   // handled by the next pass through this block
+                if (p->cp_every) checkpoint_device_batch(p, s, d, hist_seen);
+                if (h.done) break;
+                continue;
+            }
             if (p->n_inst && h.iteration >= p->inst_rows_cap) size_instance_rows(p, 2 * p->inst_rows_cap);
             h.flags = 0;
             h.exit_ctr = 0;

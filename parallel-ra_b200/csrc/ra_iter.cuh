@@ -263,9 +263,10 @@ constexpr int kClaimBatch = 4;
 constexpr u64 kPosMask = (1ull << 40) - 1;
 
 struct LoserMarks {
-    u32* mark;      // per stream position
+    u32* mark;      // per stream position (minus `base`)
     u32 epoch;      // marks of this iteration (older values mean "not a loser now")
     u64 epoch_tag;  // epoch << 40: tags below it belong to tuples from earlier iterations
+    u64 base;       // stream position of mark[0] (a slice of outer rows starts there; else 0)
 };
 
 __device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 cap, u64 k, u64 mine, u64 h, Slot cur,
@@ -279,12 +280,12 @@ __device__ __forceinline__ void claim_rest(Slot* __restrict__ t, u64 cap, u64 k,
             for (;;) {
                 if (cur.tag == mine) return;     // our own claim from an attempt being replayed
                 if (cur.tag < mine) {            // older tuple, or an earlier position this iteration
-                    lm.mark[mine & kPosMask] = lm.epoch;
+                    lm.mark[(mine & kPosMask) - lm.base] = lm.epoch;
                     return;
                 }
                 const Slot prev = atomicCAS(&t[h], cur, mineslot);
                 if (slot_eq(prev, cur)) {      // we took the slot from a later position
-                    lm.mark[cur.tag & kPosMask] = lm.epoch;
+                    lm.mark[(cur.tag & kPosMask) - lm.base] = lm.epoch;   // a later position: same slice
                     return;
                 }
                 cur = prev;
@@ -314,7 +315,7 @@ __device__ __forceinline__ void claim_batch(Slot* __restrict__ t, u64 cap, const
 
 __device__ __forceinline__ LoserMarks loser_marks(const IterCtl* c, u32* mark)
 {
-    return LoserMarks{mark, (u32)c->epoch, c->epoch << 40};
+    return LoserMarks{mark, (u32)c->epoch, c->epoch << 40, 0};
 }
 
 // ---------------------------------------------------------------------------
@@ -404,13 +405,21 @@ __global__ void __launch_bounds__(kThreads) bitmap_build_kernel(BitSeen b, const
 constexpr int kJRowsPerThread = RA_JOIN_ROWS_PER_THREAD;
 constexpr int kJRows = kThreads * kJRowsPerThread;   // outer rows per tile
 
+// One slice of a rule's outer rows (an iteration whose candidates exceed the
+// candidate buffer runs in slices): rows [lo, lo + rows) of the rule's input,
+// their candidates at buffer index 0.., stream positions from `pos`.
+struct JoinSlice {
+    u64 lo, rows, pos;
+    int on;
+};
+
 __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
                                                               int outer_shift, const u64* __restrict__ csr,
                                                               const u64* __restrict__ inner, Projection pj, int bits,
                                                               u64* __restrict__ cand, u64 cand_cap,
                                                               Slot* __restrict__ seen, u64 seen_cap,
                                                               u32* __restrict__ loser, u64* __restrict__ status,
-                                                              u64 status_cap, int tile_slot, BitSeen bs)
+                                                              u64 status_cap, int tile_slot, BitSeen bs, JoinSlice sl)
 {
     __shared__ u64 s_ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
     __shared__ u64 s_start[kJRows];    // first inner row of each outer row
@@ -419,8 +428,8 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
     __shared__ u32 s_tile;
     __shared__ u64 s_prefix;
     if (ctl->flags) return;
-    const u64 n = rows_n(ctl, outer_ref);
-    const u64* outer = rows_ptr(ctl, outer_ref);
+    const u64 n = sl.on ? sl.rows : rows_n(ctl, outer_ref);
+    const u64* outer = rows_ptr(ctl, outer_ref) + (sl.on ? sl.lo : 0);
     if (n == 0) {
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = 0;
         return;
@@ -431,11 +440,12 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
         return;
     }
     if (blockIdx.x >= ntiles) return;
-    const u64 cbase = stream_base(ctl, rule);
-    const u64 tag_base = (ctl->epoch << 40) | cbase;
+    const u64 cbase = sl.on ? 0 : stream_base(ctl, rule);   // buffer index of the first candidate
+    const u64 tag_base = (ctl->epoch << 40) | (sl.on ? sl.pos : cbase);
     const u32 tag = iter_tag(ctl, tile_slot);
     u32* ctr = tile_counter(ctl, tile_slot);
-    const LoserMarks lm = loser_marks(ctl, loser);
+    LoserMarks lm = loser_marks(ctl, loser);
+    lm.base = sl.on ? sl.pos : 0;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
         __syncthreads();
@@ -519,6 +529,27 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
             }
         }
         __syncthreads();
+    }
+}
+
+// Candidates of every tile of kJRows outer rows (the host cuts an iteration
+// whose candidates exceed the candidate buffer into slices of whole tiles).
+__global__ void __launch_bounds__(kThreads) join_tile_counts_kernel(const IterCtl* __restrict__ ctl, RowsRef outer_ref,
+                                                                    int outer_shift, const u64* __restrict__ csr,
+                                                                    u64* __restrict__ tile_cnt)
+{
+    __shared__ u64 sm[kWarps + 1];
+    const u64 n = rows_n(ctl, outer_ref);
+    const u64* outer = rows_ptr(ctl, outer_ref);
+    const u64 ntiles = (n + kJRows - 1) / kJRows;
+    for (u64 t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        u64 c = 0;
+        for (u64 i = t * kJRows + threadIdx.x; i < min(n, (t + 1) * kJRows); i += kThreads) {
+            const u64 j = outer[i] >> outer_shift;
+            c += csr[j + 1] - csr[j];
+        }
+        const u64 tot = block_reduce_sum(c, sm);
+        if (threadIdx.x == 0) tile_cnt[t] = tot;
     }
 }
 
@@ -667,6 +698,11 @@ struct SelectArgs {
     int to_log;
     int passes;               // digit histograms to accumulate (reference ids)
     u64 stage_cap;
+    // a slice of the rule's outer rows: candidates at buffer index 0; `appended` winners of
+    // this iteration already in the relation's log (earlier rules and slices), `id_appended`
+    // already numbered under the rule's tag; the iteration end runs after the last slice
+    int sliced;
+    u64 appended, id_appended;
     // instance accounting (batched programs): instance i owns values [inst_base[i], inst_base[i+1])
     const u64* inst_base;     // n_inst + 1 entries, or null
     u32 n_inst;
@@ -727,12 +763,17 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
         // (a replay then never counts a winner twice).  The new delta lands in the log
         // either way (directly, or via staging + sort).
         bool over = a.inst_base && ctl->iteration >= a.inst_iter_cap;
-        for (int s = 0; s < plan.n_rels; s++) {
-            u64 incoming = 0;
-            for (int q = 0; q < rm.n_rules_in[s]; q++) incoming += ctl->cand_n[rm.rules_in[s][q]];
-            if (!incoming) continue;
-            over = over || ctl->full_n[s] + ctl->delta_n[s] + incoming > plan.log_cap[s] ||
-                   (!a.to_log && incoming > a.stage_cap);
+        if (a.sliced) {
+            const int s = plan.rule_out[rule];
+            over = over || ctl->full_n[s] + ctl->delta_n[s] + a.appended + ctl->cand_n[rule] > plan.log_cap[s];
+        } else {
+            for (int s = 0; s < plan.n_rels; s++) {
+                u64 incoming = 0;
+                for (int q = 0; q < rm.n_rules_in[s]; q++) incoming += ctl->cand_n[rm.rules_in[s][q]];
+                if (!incoming) continue;
+                over = over || ctl->full_n[s] + ctl->delta_n[s] + incoming > plan.log_cap[s] ||
+                       (!a.to_log && incoming > a.stage_cap);
+            }
         }
         if (over) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
@@ -744,15 +785,20 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
     if (active && c > 0 && blockIdx.x < ntiles) {
         // destination offset and intern base: winners of earlier rules into the same relation / tag
         u64 dst_off = 0, id_ctr = ctl->intern[tslot];
-        for (int q = 0; q < rule; q++) {
-            if (plan.rule_out[q] == out) dst_off += ctl->win_n[q];
-            if (plan.rule_tag[q] == tslot) id_ctr += ctl->win_n[q];
+        if (a.sliced) {
+            dst_off = a.appended;
+            id_ctr += a.id_appended;
+        } else {
+            for (int q = 0; q < rule; q++) {
+                if (plan.rule_out[q] == out) dst_off += ctl->win_n[q];
+                if (plan.rule_tag[q] == tslot) id_ctr += ctl->win_n[q];
+            }
         }
         u64* dk = a.dst_keys;
         u64* dv = a.dst_ids;
         if (a.to_log) dst_off += ctl->full_n[out] + ctl->delta_n[out];
         const u64 tag_word = plan.rel_tag_word[out];
-        const u64 cbase = stream_base(ctl, rule);
+        const u64 cbase = a.sliced ? 0 : stream_base(ctl, rule);
         const u32 ep = (u32)ctl->epoch;
         const u64* in = cand + cbase;
         const u32 tag = iter_tag(ctl, tile_slot);

@@ -310,7 +310,7 @@ __device__ void p_join(const PersistArgs& A, int q, PJoinSmem& sm, int tslot)
     const u64 epoch = ldcg(&c->epoch);
     const u64 ep40 = epoch << 40;
     const u32 tag = p_iter_tag(ldcg(&c->iteration), tslot);
-    const LoserMarks lm{A.loser, (u32)epoch, ep40};
+    const LoserMarks lm{A.loser, (u32)epoch, ep40, 0};
     const u64* __restrict__ csr = R.csr;
     const u64* __restrict__ inner = R.inner;
     // chunks dealt out statically (warp w: w, w + W, ...); every warp is resident, so a
@@ -429,7 +429,7 @@ __device__ void p_heavy(const PersistArgs& A, u64 items)
     const int lane = threadIdx.x & 31;
     const u64 epoch = ldcg(&c->epoch);
     const u64 ep40 = epoch << 40;
-    const LoserMarks lm{A.loser, (u32)epoch, ep40};
+    const LoserMarks lm{A.loser, (u32)epoch, ep40, 0};
     for (;;) {
         u64 it = 0;
         if (lane == 0) it = atomicAdd(&c->heavy_ctr, 1u);
@@ -476,7 +476,7 @@ __device__ void p_copy(const PersistArgs& A, int q)
     const u64* __restrict__ in = p_rows_ptr(c, R.in);
     const u64 epoch = ldcg(&c->epoch);
     const u64 tag_base = (epoch << 40) | cbase;
-    const LoserMarks lm{A.loser, (u32)epoch, epoch << 40};
+    const LoserMarks lm{A.loser, (u32)epoch, epoch << 40, 0};
     u64* out = A.cand + cbase;
     const u64 stride = (u64)gridDim.x * kThreads * kPClaim;
     for (u64 p0 = (u64)blockIdx.x * kThreads * kPClaim; p0 < n; p0 += stride) {

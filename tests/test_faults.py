@@ -37,7 +37,9 @@ def test_injected_out_of_memory_then_recovery(dense, where):
     holds at its peak stops it after the first SCC has run -- the next run must run every
     SCC again (the history holds both)."""
     rows = tc_rows(3000, 4500, 7)
-    p = P.Program(0)
+    # the hash-set variant numbers ids in the reference's order: that path does not run an
+    # iteration in slices, so a cap below its buffers fails the run (test_sliced_* covers slices)
+    p = P.Program(0, id_order=None if dense else P.engine.IDS_REFERENCE)
     if not dense:
         p.set_tuning(dense_max_bytes=0)
     rels = P.programs.build_tc(p, rows)
@@ -96,3 +98,47 @@ def test_corrupt_size_metadata_is_rejected(tmp_path):
     os.remove(path + ".size")
     with pytest.raises(P.RAError):
         p.load_file(G, path)
+
+
+def layered_graph(a, b, c):
+    """Sources 0..a-1 -> every hub a..a+b-1 -> every target: one join iteration derives
+    each (source, target) pair b times -- a * b * c candidates for a * c new tuples."""
+    src = np.arange(a, dtype=np.uint64)
+    hub = np.arange(a, a + b, dtype=np.uint64)
+    tgt = np.arange(a + b, a + b + c, dtype=np.uint64)
+    e1 = np.stack(np.meshgrid(src, hub, indexing="ij"), axis=-1).reshape(-1, 2)
+    e2 = np.stack(np.meshgrid(hub, tgt, indexing="ij"), axis=-1).reshape(-1, 2)
+    return P.datagen.with_row_ids(np.concatenate([e1, e2]))
+
+
+def test_sliced_iteration_under_a_memory_cap():
+    """An iteration whose candidates (9M: 216 MB of candidate buffer and marks at the
+    engine's 2x growth) exceed what the cap leaves -- 100 MB below the uncapped run's
+    peak -- runs in slices of outer rows: same history and tuples as the oracle, and
+    the same log, ids included, as the uncapped run."""
+    rows = layered_graph(300, 100, 300)
+    o = O.OracleProgram()
+    orels = P.programs.build_tc(o, rows)
+    o.execute(1)
+
+    def run(cap):
+        p = P.Program(0)
+        p.set_tuning(dense_max_bytes=0)   # the hash-set path (the dense evaluator would take 700 values)
+        p.set_evaluators(reach=False)
+        p.set_memory_cap(cap)
+        rels = P.programs.build_tc(p, rows)
+        p.execute(1)
+        return p, rels
+
+    free, fr = run(0)
+    cap = free.stats().device_bytes_peak - (100 << 20)
+    capped, cr = run(cap)
+    st = capped.stats()
+    assert st.sliced_iterations >= 1 and st.sliced_passes >= 2
+    assert st.device_bytes_peak <= cap
+    assert capped.history() == o.history()
+    got = capped.dump_full(cr["T"])
+    assert np.array_equal(got[:, :2], o.dump_full(orels["T"])[:, :2])
+    assert np.array_equal(got, free.dump_full(fr["T"]))   # the same log, ids included
+    assert free.stats().sliced_iterations == 0
+
