@@ -115,6 +115,8 @@ typedef struct ra_stats {
     uint64_t sliced_iterations; /* iterations run in slices of outer rows: their candidates did not fit
                                    the candidate buffer the memory cap (ra_program_set_memory_cap) allows */
     uint64_t sliced_passes;     /* join + select passes of those iterations */
+    uint64_t heavy_items;       /* work items (2048 candidates each) that join rows with more than 4096
+                                   matches were split into, expanded by every block of the launch */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose

@@ -118,6 +118,8 @@ struct Relation {
     u64* csr_delta = nullptr;
     u64 csr_delta_version = ~0ull;
     u64 csr_delta_cap = 0;
+    u64 csr_full_longest = 0;      // most rows sharing one join key, per CSR
+    u64 csr_delta_longest = 0;
     // bitmap seen set (binary relations over small domains), kept between runs
     u32* bm_seen = nullptr;
     u32* bm_fresh = nullptr;
@@ -209,8 +211,9 @@ struct ra_program {
     u64* sort_v[2] = {};
     u64* status = nullptr;
     u64 status_cap = 0;
-    HeavyItem* dheavy = nullptr;  // heavy-row work items of the persistent SCC kernel
+    HeavyItem* dheavy = nullptr;  // heavy-row work items of the join launches
     u64 heavy_cap = 0;
+    u64 heavy_cands = 0;          // candidates of an iteration the heavy list must cover (bitmap rules write none)
     // instances (batched programs): instance i owns values [inst_base_h[i], inst_base_h[i + 1])
     std::vector<u64> inst_base_h;  // n_inst + 1 entries, the last ~0
     u64* dinst_base = nullptr;
@@ -531,7 +534,8 @@ void version_rows(ra_program* p, Relation& r, int ver, const u64** k, const u64*
     *n = r.full_n;
 }
 
-// CSR offsets (2^(jcc*W) + 1 entries) over the join key of a version's rows
+// CSR offsets (2^(jcc*W) + 1 entries) over the join key of a version's rows;
+// its longest row (most rows sharing one key) goes to csr_{full,delta}_longest
 const u64* version_csr(ra_program* p, Relation& r, int ver)
 {
     const int jbits = (int)r.jcc * p->bits;
@@ -545,10 +549,10 @@ const u64* version_csr(ra_program* p, Relation& r, int ver)
     if (*slot && *stamp == want) return *slot;
     // the key width changes with the values loaded: a reloaded program may need a larger index
     const u64 nk = (1ull << jbits) + 1;
-    if (*cap < nk) {
+    if (*cap < nk + 1) {
         dev_free(p, slot);
-        dev_alloc(p, slot, nk);
-        *cap = nk;
+        dev_alloc(p, slot, nk + 1);
+        *cap = nk + 1;
     }
     const u64 *k, *v;
     u64 n;
@@ -561,6 +565,10 @@ const u64* version_csr(ra_program* p, Relation& r, int ver)
         LAUNCHED();
     }
     scan_exclusive<u32>(p, counts, nk, *slot, false);
+    CK(cudaMemsetAsync(*slot + nk, 0, 8, p->stream));
+    csr_row_max<<<grid_for(nk), kThreads, 0, p->stream>>>(counts, nk, (unsigned long long*)(*slot + nk));
+    LAUNCHED();
+    (ver == RA_DELTA ? r.csr_delta_longest : r.csr_full_longest) = read_scalar(p, *slot + nk);
     dev_free(p, &counts);
     *stamp = want;
     return *slot;
@@ -898,6 +906,7 @@ struct DevRule {
     RowsRef in;            // join: outer rows; copy: input rows
     Projection pj;
     const u64* csr = nullptr;
+    u64 longest = 0;                // join: the inner CSR's longest row (heavy-row split above kHeavyRow)
     const u64* inner = nullptr;
     int outer_shift = 0;
     int pred = 0;
@@ -997,6 +1006,7 @@ bool build_dev_scc(ra_program* p, Scc& s, DevScc& d)
             version_rows(p, in, jp.inner_ver, &ik, &iv, &inn);
             dr.inner = ik;
             dr.csr = version_csr(p, in, jp.inner_ver);
+            dr.longest = jp.inner_ver == RA_DELTA ? in.csr_delta_longest : in.csr_full_longest;
             dr.pj = jp.pj;
             const Relation& o = p->rels[jp.outer_rel];
             dr.outer_shift = (int)(o.arity - o.jcc) * p->bits;
@@ -1081,7 +1091,8 @@ void dev_size_buffers(ra_program* p, DevScc& d, u64 cand_cap, u64 stage_cap, u64
         p->status_cap = st_need;
     }
     // heavy-row slices: at most one per kHeavyPiece candidates plus one per heavy row
-    const u64 heavy_need = p->dcand_cap / kHeavyPiece + p->dcand_cap / kHeavyRow + 64;
+    const u64 heavy_cands = std::max(p->dcand_cap, p->heavy_cands);
+    const u64 heavy_need = heavy_cands / kHeavyPiece + heavy_cands / kHeavyRow + 64;
     if (heavy_need > p->heavy_cap) {
         dev_free(p, &p->dheavy);
         p->heavy_cap = 0;
@@ -1127,6 +1138,13 @@ void size_instance_rows(ra_program* p, u64 rows)
     p->inst_rows_cap = rows;
 }
 
+// The fused join of a rule: with the heavy-row list when its inner CSR has a
+// row longer than kHeavyRow (a skewed key), else the plain tile loop.
+decltype(&join_fused_kernel<false>) join_kernel(const DevRule& r)
+{
+    return r.longest > kHeavyRow ? join_fused_kernel<true> : join_fused_kernel<false>;
+}
+
 // per-launch events (diagnostic mode only; never inside a graph capture)
 struct PhaseTimer {
     ra_program* p;
@@ -1161,10 +1179,11 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
         PhaseTimer pt(p, 2);
         if (r.kind == kJoin)
-            join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
-                                                             p->bits, p->dcand, p->dcand_cap, out.seen,
-                                                             out.seen_cap, p->dloser, p->status, p->status_cap,
-                                                             slot++, d.bit[r.out_slot], JoinSlice{0, 0, 0, 0});
+            join_kernel(r)<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
+                                                          p->bits, p->dcand, p->dcand_cap, out.seen, out.seen_cap,
+                                                          p->dloser, p->status, p->status_cap, slot++,
+                                                          d.bit[r.out_slot], JoinSlice{0, 0, 0, 0}, p->dheavy,
+                                                          p->heavy_cap);
         else
             copy_claim_kernel<<<2 * G, kThreads, 0, p->stream>>>(p->ctl, pl, q, r.in, r.pj, p->bits, r.pred,
                                                                  p->dcand, p->dcand_cap, out.seen, out.seen_cap,
@@ -1659,10 +1678,11 @@ void run_sliced_iteration(ra_program* p, Scc& s, DevScc& d)
             CK(cudaMemsetAsync(p->dloser, 0, std::max<u64>(c, 1) * 4, p->stream));
             CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
             CK(cudaMemsetAsync(p->ctl->tile_ctr, 0, sizeof(p->ctl->tile_ctr), p->stream));
-            join_fused_kernel<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
-                                                             p->bits, p->dcand, p->dcand_cap, out.seen, out.seen_cap,
-                                                             p->dloser, p->status, p->status_cap, 0, d.bit[r.out_slot],
-                                                             JoinSlice{lo, rows, pos + rule_pos, 1});
+            join_kernel(r)<<<G, kThreads, 0, p->stream>>>(p->ctl, q, r.in, r.outer_shift, r.csr, r.inner, r.pj,
+                                                          p->bits, p->dcand, p->dcand_cap, out.seen, out.seen_cap,
+                                                          p->dloser, p->status, p->status_cap, 0, d.bit[r.out_slot],
+                                                          JoinSlice{lo, rows, pos + rule_pos, 1}, p->dheavy,
+                                                          p->heavy_cap);
             LAUNCHED();
             SelectArgs a{};
             a.rule = q;
@@ -1698,7 +1718,7 @@ void run_sliced_iteration(ra_program* p, Scc& s, DevScc& d)
         h.cand_n[q] = cand_tot[q];
         h.win_n[q] = win_tot[q];
     }
-    for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
+    for (int i = 0; i < 2 * kBankWords; i++) h.tile_ctr[i] = 0;
     CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
     CK(cudaMemsetAsync(p->status, 0, p->status_cap * 8, p->stream));
     iter_end_kernel<<<64, kThreads, 0, p->stream>>>(p->ctl, pl, d.rm, p->dhist, 0, 0);
@@ -1923,6 +1943,11 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             }
             refresh_refs(p, d);
             const bool cand_short = replay && total > p->dcand_cap;
+            if (replay) {   // the heavy-row list covers every rule's candidates, bitmap rules' included
+                u64 all = 0;
+                for (int q = 0; q < pl.n_rules; q++) all += h.cand_n[q];
+                p->heavy_cands = std::max(p->heavy_cands, 2 * all);
+            }
             try {
                 dev_size_buffers(p, d, replay ? std::max(p->dcand_cap, 2 * total) : p->dcand_cap,
                                  replay ? std::max(p->stage_cap, 2 * stage_need) : p->stage_cap,
@@ -1945,7 +1970,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 h.flags = 0;
                 h.exit_ctr = 0;
                 h.bar_count = 0;
-                for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
+                for (int i = 0; i < 2 * kBankWords; i++) h.tile_ctr[i] = 0;
                 CK(cudaMemcpyAsync(p->ctl, p->hctl, ctl_header_bytes(), cudaMemcpyHostToDevice, p->stream));
                 run_sliced_iteration(p, s, d);
                 if (h.flags & kFlagGrow) continue;   // handled by the next pass through this block
@@ -1958,7 +1983,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
             h.exit_ctr = 0;
             h.bar_count = 0;
             if (replay) {
-                for (int i = 0; i < 2 * kTileSlots; i++) h.tile_ctr[i] = 0;
+                for (int i = 0; i < 2 * kBankWords; i++) h.tile_ctr[i] = 0;
                 h.heavy_n = 0;
                 h.heavy_ctr = 0;
             }
@@ -2023,6 +2048,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     p->epoch = h.epoch;
     p->stats.iterations += h.iteration;
     p->stats.join_candidates += h.candidates;
+    p->stats.heavy_items += h.heavy_items;
     p->stats.new_tuples += h.new_tuples;
     p->stats.kernel_launches += (u64)body_kernels * h.iteration;
     p->stats.dedup_launches += (u64)d.rules.size() * h.iteration;

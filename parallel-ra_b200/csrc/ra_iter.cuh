@@ -33,6 +33,8 @@ constexpr int kMaxSccRules = 8;
 constexpr int kMaxTagSlots = 8;
 constexpr int kMaxPasses = 8;
 constexpr int kTileSlots = 128;
+// a bank of launch counters: kTileSlots tile counters, then 3 heavy-row counters per rule
+constexpr int kBankWords = kTileSlots + 3 * kMaxSccRules;
 
 // flags
 constexpr u32 kFlagOverflow = 1u;   // a buffer is too small: replay the iteration after growing it
@@ -55,7 +57,7 @@ struct IterCtl {
     u64 runs[kMaxSccRels];  // non-empty deltas moved into full (sorted runs added)
     u64 t_start;                    // %globaltimer when the SCC started (ns)
     u64 time_cap;                   // entries of the per-iteration end-time buffer
-    u32 tile_ctr[2 * kTileSlots];   // two banks: iteration k uses bank k & 1
+    u32 tile_ctr[2 * kBankWords];   // two banks: iteration k uses bank k & 1
     u32 exit_ctr;                   // blocks of the running select launch that have finished
     u32 flags;
     u32 done;
@@ -70,6 +72,7 @@ struct IterCtl {
     u32 bar_flags;                  // flags / done / heavy_n as the last arriver saw them
     u32 bar_done;
     u64 bar_heavy;
+    u64 heavy_items;                // heavy-row work items pushed in this SCC (both paths)
     u64 sort_hist[kMaxSccRels][kMaxPasses][kRadix];
 };
 
@@ -225,7 +228,7 @@ __device__ __forceinline__ u32 iter_tag(const IterCtl* c, int slot)
 
 __device__ __forceinline__ u32* tile_counter(IterCtl* c, int slot)
 {
-    return &c->tile_ctr[(c->iteration & 1) * kTileSlots + slot];
+    return &c->tile_ctr[(c->iteration & 1) * kBankWords + slot];
 }
 
 // first index i in [0, n) with a[i] > x (n if none)
@@ -413,48 +416,91 @@ struct JoinSlice {
     int on;
 };
 
-__global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
-                                                              int outer_shift, const u64* __restrict__ csr,
-                                                              const u64* __restrict__ inner, Projection pj, int bits,
-                                                              u64* __restrict__ cand, u64 cand_cap,
-                                                              Slot* __restrict__ seen, u64 seen_cap,
-                                                              u32* __restrict__ loser, u64* __restrict__ status,
-                                                              u64 status_cap, int tile_slot, BitSeen bs, JoinSlice sl)
+// Skewed keys.  An outer row with more than kHeavyRow matches is not expanded
+// by its tile's block: it keeps its stream positions, and the tile pushes it as
+// work items of kHeavyPiece candidates that every warp of the grid takes from a
+// shared list once all tiles have been scanned.
+constexpr u64 kHeavyRow = 4096;
+constexpr u64 kHeavyPiece = 2048;
+
+// One heavy row's slice of candidates: stream positions [pos, pos + count).
+struct __align__(16) HeavyItem {
+    u64 pos;     // stream position of the first candidate (relative to the launch's first)
+    u64 key;     // the outer row
+    u64 start;   // its first inner row of the slice
+    u32 count;
+    u32 rule;
+};
+static_assert(sizeof(HeavyItem) == 32, "HeavyItem is read as two 16-byte words");
+
+__device__ __forceinline__ u32 ldcg_u32(const u32* p) { return __ldcg(p); }
+__device__ __forceinline__ HeavyItem ldcg_item(const HeavyItem* p)
 {
-    __shared__ u64 s_ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
-    __shared__ u64 s_start[kJRows];    // first inner row of each outer row
-    __shared__ u64 s_key[kJRows];      // outer keys
-    __shared__ u64 sm[kWarps + 1];
-    __shared__ u32 s_tile;
-    __shared__ u64 s_prefix;
-    if (ctl->flags) return;
-    const u64 n = sl.on ? sl.rows : rows_n(ctl, outer_ref);
-    const u64* outer = rows_ptr(ctl, outer_ref) + (sl.on ? sl.lo : 0);
-    if (n == 0) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = 0;
-        return;
-    }
+    const ulonglong2 a = __ldcg((const ulonglong2*)p), b = __ldcg((const ulonglong2*)p + 1);
+    HeavyItem h;
+    h.pos = a.x;
+    h.key = a.y;
+    h.start = b.x;
+    h.count = (u32)b.y;
+    h.rule = (u32)(b.y >> 32);
+    return h;
+}
+
+// Per-rule counters of the heavy-row list, banked with the tile counters.
+enum HeavyWord { kHvItems = 0, kHvScanned = 1, kHvTaken = 2 };
+__device__ __forceinline__ u32* heavy_counter(IterCtl* c, int rule, int w)
+{
+    return &c->tile_ctr[(c->iteration & 1) * kBankWords + kTileSlots + 3 * rule + w];
+}
+
+// Shared memory of one join block.
+struct JoinSmem {
+    u64 ex[kJRows + 1];   // exclusive prefix of match counts inside the tile
+    u32 lx[kJRows + 1];   // the same over the rows this block expands (kSplit: heavy rows count 0)
+    u64 start[kJRows];    // first inner row of each outer row
+    u64 key[kJRows];      // outer keys
+    u64 sm[kWarps + 1];
+    u32 tile;
+    u64 prefix, hbase, hn;
+};
+
+// The tiles of one join launch.  kSplit: the inner CSR has rows longer than
+// kHeavyRow, so a tile's heavy rows go to the shared list and every block
+// expands that list after the tiles; without it the code is the plain tile loop.
+template <bool kSplit>
+__device__ __forceinline__ void join_tiles(JoinSmem& S, IterCtl* __restrict__ ctl, int rule, const u64* __restrict__ outer,
+                                           u64 n, int outer_shift, const u64* __restrict__ csr,
+                                           const u64* __restrict__ inner, const Projection& pj, int bits,
+                                           u64* __restrict__ cand, u64 cand_cap, Slot* __restrict__ seen,
+                                           u64 seen_cap, u32* __restrict__ loser, u64* __restrict__ status,
+                                           int tile_slot, const BitSeen& bs, const JoinSlice& sl,
+                                           HeavyItem* __restrict__ heavy, u64 heavy_cap)
+{
     const u64 ntiles = (n + kJRows - 1) / kJRows;
-    if (ntiles > status_cap) {   // the host sizes status for the largest outer input: never taken
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagStatus);
-        return;
-    }
-    if (blockIdx.x >= ntiles) return;
+    if (!kSplit && blockIdx.x >= ntiles) return;
     const u64 cbase = sl.on ? 0 : stream_base(ctl, rule);   // buffer index of the first candidate
     const u64 tag_base = (ctl->epoch << 40) | (sl.on ? sl.pos : cbase);
     const u32 tag = iter_tag(ctl, tile_slot);
     u32* ctr = tile_counter(ctl, tile_slot);
     LoserMarks lm = loser_marks(ctl, loser);
     lm.base = sl.on ? sl.pos : 0;
+    if (kSplit && threadIdx.x == 0) {   // heavy items of the earlier rules of this iteration come first
+        u64 b = 0;
+        for (int r = 0; r < rule; r++) b += *heavy_counter(ctl, r, kHvItems);
+        S.hbase = b;
+    }
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(ctr, 1u);
+        // (kSplit) a block beyond the tiles that sees every tile taken needs no atomic
+        if (threadIdx.x == 0)
+            S.tile = (kSplit && blockIdx.x >= ntiles && ldcg_u32(ctr) >= (u32)ntiles) ? (u32)ntiles
+                                                                                     : atomicAdd(ctr, 1u);
         __syncthreads();
-        const u64 tile = s_tile;
+        const u64 tile = S.tile;
         __syncthreads();
         if (tile >= ntiles) break;
         const u64 r0 = tile * kJRows;
         u64 cnt[kJRowsPerThread];
-        u64 local = 0;
+        u64 local = 0;   // kSplit: (all matches << 24) | matches of the rows expanded here
 #pragma unroll
         for (int k = 0; k < kJRowsPerThread; k++) {
             const int li = threadIdx.x * kJRowsPerThread + k;
@@ -465,59 +511,104 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                 const u64 j = key >> outer_shift;
                 const u64 s = csr[j];
                 cnt[k] = csr[j + 1] - s;
-                s_start[li] = s;
-                s_key[li] = key;
+                S.start[li] = s;
+                S.key[li] = key;
             }
-            local += cnt[k];
+            local += kSplit ? ((cnt[k] << 24) | (cnt[k] > kHeavyRow ? 0 : cnt[k])) : cnt[k];
         }
-        u64 agg;
-        u64 ex = block_exclusive_scan(local, sm, &agg);
+        u64 aggp;
+        u64 ex = block_exclusive_scan(local, S.sm, &aggp);
+        bool mine_heavy = false;
 #pragma unroll
         for (int k = 0; k < kJRowsPerThread; k++) {
-            s_ex[threadIdx.x * kJRowsPerThread + k] = ex;
-            ex += cnt[k];
+            const int li = threadIdx.x * kJRowsPerThread + k;
+            if (kSplit) {
+                S.ex[li] = ex >> 24;
+                S.lx[li] = (u32)(ex & 0xffffffu);
+                ex += (cnt[k] << 24) | (cnt[k] > kHeavyRow ? 0 : cnt[k]);
+                mine_heavy |= cnt[k] > kHeavyRow;
+            } else {
+                S.ex[li] = ex;
+                ex += cnt[k];
+            }
         }
-        if (threadIdx.x == 0) s_ex[kJRows] = agg;
+        const u64 agg = kSplit ? aggp >> 24 : aggp, lagg = kSplit ? aggp & 0xffffffu : aggp;
+        if (threadIdx.x == 0) {
+            S.ex[kJRows] = agg;
+            if (kSplit) S.lx[kJRows] = (u32)lagg;
+        }
         if (threadIdx.x < 32) {
             const u64 pre = lookback_warp(status, (u32)tile, agg, tag, &ctl->flags);
-            if (threadIdx.x == 0) s_prefix = pre;
+            if (threadIdx.x == 0) S.prefix = pre;
         }
         __syncthreads();
-        const u64 prefix = s_prefix;
+        const u64 prefix = S.prefix;
         if (tile == ntiles - 1 && threadIdx.x == 0) {
             ctl->cand_n[rule] = prefix + agg;
             ctl->outer_rows += n;
         }
-        if (!bs.seen && cbase + prefix + agg > cand_cap) {
-            if (threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
-        } else {
-            // the tile's candidates: position prefix + j, j in [0, agg)
+        const bool room = bs.seen || cbase + prefix + agg <= cand_cap;
+        if (!room && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagOverflow);
+        if (kSplit) {
+            if (room && mine_heavy) {
+#pragma unroll
+                for (int k = 0; k < kJRowsPerThread; k++) {
+                    if (cnt[k] <= kHeavyRow) continue;
+                    const int li = threadIdx.x * kJRowsPerThread + k;
+                    const u64 pieces = (cnt[k] + kHeavyPiece - 1) / kHeavyPiece;
+                    const u64 at = S.hbase + atomicAdd(heavy_counter(ctl, rule, kHvItems), (u32)pieces);
+                    if (at + pieces > heavy_cap) {
+                        atomicOr(&ctl->flags, kFlagOverflow);
+                        continue;
+                    }
+                    const u64 p0 = prefix + S.ex[li];
+                    for (u64 pc = 0; pc < pieces; pc++) {
+                        const u64 off = pc * kHeavyPiece;
+                        heavy[at + pc] = HeavyItem{p0 + off, S.key[li], S.start[li] + off,
+                                                   (u32)min(kHeavyPiece, cnt[k] - off), (u32)rule};
+                    }
+                    atomicAdd((unsigned long long*)&ctl->heavy_items, (unsigned long long)pieces);
+                }
+                __threadfence();
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(heavy_counter(ctl, rule, kHvScanned), 1u);
+        }
+        if (room) {
+            // the tile's candidates expanded here: position prefix + ex[row] + rank
             const u64 nr = min((u64)kJRows, n - r0);
-            for (u64 j0 = 0; j0 < agg; j0 += (u64)kThreads * kClaimBatch) {
+            for (u64 j0 = 0; j0 < lagg; j0 += (u64)kThreads * kClaimBatch) {
                 u64 key[kClaimBatch], mine[kClaimBatch];
                 bool valid[kClaimBatch];
                 u64 ik[kClaimBatch];
+                u64 at[kClaimBatch];
                 int rr[kClaimBatch];
-                u64 rank[kClaimBatch];
 #pragma unroll
                 for (int k = 0; k < kClaimBatch; k++) {
                     const u64 j = j0 + threadIdx.x + (u64)k * kThreads;
-                    valid[k] = j < agg;
+                    valid[k] = j < lagg;
                     rr[k] = 0;
-                    rank[k] = 0;
+                    at[k] = 0;
                     ik[k] = 0;
                     if (valid[k]) {
-                        rr[k] = (int)upper_bound_dev(s_ex, nr, j) - 1;
-                        rank[k] = j - s_ex[rr[k]];
-                        ik[k] = inner[s_start[rr[k]] + rank[k]];
+                        u64 rank;
+                        if (!kSplit || lagg == agg) {   // no heavy row in the tile: j is the position
+                            rr[k] = (int)upper_bound_dev(S.ex, nr, j) - 1;
+                            rank = j - S.ex[rr[k]];
+                            at[k] = prefix + j;
+                        } else {
+                            rr[k] = (int)upper_bound_dev(S.lx, nr, j) - 1;
+                            rank = j - S.lx[rr[k]];
+                            at[k] = prefix + S.ex[rr[k]] + rank;
+                        }
+                        ik[k] = inner[S.start[rr[k]] + rank];
                     }
                 }
 #pragma unroll
                 for (int k = 0; k < kClaimBatch; k++) {
-                    const u64 j = j0 + threadIdx.x + (u64)k * kThreads;
-                    key[k] = valid[k] ? project(pj, s_key[rr[k]], ik[k], bits) : 0;
-                    mine[k] = tag_base + prefix + j;
-                    if (valid[k] && !bs.seen) cand[cbase + prefix + j] = key[k];
+                    key[k] = valid[k] ? project(pj, S.key[rr[k]], ik[k], bits) : 0;
+                    mine[k] = tag_base + at[k];
+                    if (valid[k] && !bs.seen) cand[cbase + at[k]] = key[k];
                 }
                 if (bs.seen) {
 #pragma unroll
@@ -530,6 +621,93 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
         }
         __syncthreads();
     }
+    if (!kSplit) return;
+    // Heavy rows.  This block saw every tile taken, each by a running block that
+    // scans (and pushes) its tile before expanding it, so the wait ends once the
+    // last tile's look-back has; bounded all the same.
+    if (threadIdx.x == 0) {
+        u64 spins = 0;
+        const u32* scanned = heavy_counter(ctl, rule, kHvScanned);
+        while (ldcg_u32(scanned) < (u32)ntiles) {
+            if (++spins > kSpinLimit) {
+                atomicOr(&ctl->flags, kFlagTimeout);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+        // a push that found the list full reserved items it never wrote: the
+        // iteration is replayed with more room, so nothing is taken
+        const u64 items = ldcg_u32(heavy_counter(ctl, rule, kHvItems));
+        const bool bad = spins > kSpinLimit || (ldcg_u32(&ctl->flags) & (kFlagOverflow | kFlagTimeout)) ||
+                         S.hbase + items > heavy_cap;
+        S.hn = bad ? 0 : items;
+    }
+    __syncthreads();
+    const u64 hn = S.hn;
+    if (hn == 0) return;
+    const int lane = threadIdx.x & 31;
+    u32* taken = heavy_counter(ctl, rule, kHvTaken);
+    for (;;) {
+        u32 it = 0;
+        if (lane == 0) it = atomicAdd(taken, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= hn) break;
+        const HeavyItem h = ldcg_item(&heavy[S.hbase + it]);
+        for (u32 t0 = 0; t0 < h.count; t0 += 32 * kClaimBatch) {
+            u64 key[kClaimBatch], mine[kClaimBatch], ik[kClaimBatch];
+            bool valid[kClaimBatch];
+#pragma unroll
+            for (int b = 0; b < kClaimBatch; b++) {
+                const u32 t = t0 + (u32)b * 32 + lane;
+                valid[b] = t < h.count;
+                ik[b] = valid[b] ? inner[h.start + t] : 0;
+            }
+#pragma unroll
+            for (int b = 0; b < kClaimBatch; b++) {
+                const u64 at = h.pos + t0 + (u64)b * 32 + lane;
+                key[b] = valid[b] ? project(pj, h.key, ik[b], bits) : 0;
+                mine[b] = tag_base + at;
+                if (valid[b] && !bs.seen) cand[cbase + at] = key[b];
+            }
+            if (bs.seen) {
+#pragma unroll
+                for (int b = 0; b < kClaimBatch; b++)
+                    if (valid[b]) bit_claim(bs, key[b], bits, &ctl->flags);
+            } else {
+                claim_batch(seen, seen_cap, key, mine, valid, lm, &ctl->flags);
+            }
+        }
+    }
+}
+
+// One join rule's launch.  kSplit (the host's choice: the inner CSR has a row
+// longer than kHeavyRow) adds the heavy-row list; otherwise the plain tile loop.
+template <bool kSplit>
+__global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kernel(IterCtl* __restrict__ ctl, int rule, RowsRef outer_ref,
+                                                              int outer_shift, const u64* __restrict__ csr,
+                                                              const u64* __restrict__ inner, Projection pj, int bits,
+                                                              u64* __restrict__ cand, u64 cand_cap,
+                                                              Slot* __restrict__ seen, u64 seen_cap,
+                                                              u32* __restrict__ loser, u64* __restrict__ status,
+                                                              u64 status_cap, int tile_slot, BitSeen bs, JoinSlice sl,
+                                                              HeavyItem* __restrict__ heavy, u64 heavy_cap)
+{
+    __shared__ JoinSmem S;
+    if (ctl->flags) return;
+    const u64 n = sl.on ? sl.rows : rows_n(ctl, outer_ref);
+    const u64* outer = rows_ptr(ctl, outer_ref) + (sl.on ? sl.lo : 0);
+    if (n == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = 0;
+        return;
+    }
+    const u64 ntiles = (n + kJRows - 1) / kJRows;
+    if (ntiles > status_cap) {   // the host sizes status for the largest outer input: never taken
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->flags, kFlagStatus);
+        return;
+    }
+    join_tiles<kSplit>(S, ctl, rule, outer, n, outer_shift, csr, inner, pj, bits, cand, cand_cap, seen, seen_cap,
+                       loser, status, tile_slot, bs, sl, heavy, heavy_cap);
 }
 
 // Candidates of every tile of kJRows outer rows (the host cuts an iteration
@@ -676,7 +854,7 @@ __device__ void end_of_iteration(IterCtl* __restrict__ ctl, const SccPlan& plan,
             cont = false;
         }
         // the next iteration's bank of tile counters (used last by the previous iteration)
-        for (int i = 0; i < kTileSlots; i++) ctl->tile_ctr[(ctl->iteration & 1) * kTileSlots + i] = 0;
+        for (int i = 0; i < kBankWords; i++) ctl->tile_ctr[(ctl->iteration & 1) * kBankWords + i] = 0;
         ctl->heavy_n = 0;
         ctl->heavy_ctr = 0;
     }

@@ -119,6 +119,18 @@ __global__ void __launch_bounds__(kThreads) csr_count(const u64* __restrict__ ke
         atomicAdd(&counts[keys[i] >> shift], 1u);
 }
 
+// The longest CSR row (most rows sharing one join key), stored after the offsets:
+// the fused join reads it to skip its skewed-key machinery when no row can be heavy.
+__global__ void __launch_bounds__(kThreads) csr_row_max(const u32* __restrict__ counts, u64 n,
+                                                        unsigned long long* __restrict__ out)
+{
+    u32 m = 0;
+    for (u64 i = (u64)blockIdx.x * kThreads + threadIdx.x; i < n; i += (u64)gridDim.x * kThreads)
+        m = max(m, counts[i]);
+    for (int d = 16; d > 0; d >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, d));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, (unsigned long long)m);
+}
+
 // ---------------------------------------------------------------------------
 // Join expansion.  Outer rows in trie order; for outer row i the matches are
 // inner rows [start, start+cnt).  cnt[i] feeds an exclusive scan giving each

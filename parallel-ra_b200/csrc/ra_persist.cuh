@@ -46,8 +46,6 @@ constexpr int kPJChunk = 32 * kPRowsPerLane;   // outer rows per warp chunk
 constexpr int kPSelPerLane = 8;
 constexpr int kPSChunk = 32 * kPSelPerLane;    // candidates per warp chunk of the select
 constexpr int kPClaim = 4;                     // claims in flight per lane
-constexpr u64 kHeavyRow = 4096;                // a row with more matches is expanded as work items
-constexpr u64 kHeavyPiece = 2048;              // candidates per work item
 // a grid barrier gives up after this long (a legitimate phase of one iteration is
 // far shorter; the limit only ends a wait that could otherwise never finish)
 constexpr u64 kBarrierNs = 4000000000ull;
@@ -116,15 +114,6 @@ __device__ u64 p_lookback(u64* status, u32 tile, u64 agg, u32 tag, u32* flags)
         atomicExch((unsigned long long*)&status[tile], (unsigned long long)st_pack(tag, kStIncl, excl + agg));
     return excl;
 }
-
-// One heavy row's slice of candidates: stream positions [pos, pos + count).
-struct HeavyItem {
-    u64 pos;     // absolute stream position of the first candidate
-    u64 key;     // the outer row
-    u64 start;   // its first inner row of the slice
-    u32 count;
-    u32 rule;
-};
 
 struct PRule {
     int kind;             // kJoinRule, or a copy kind
@@ -385,6 +374,7 @@ __device__ void p_join(const PersistArgs& A, int q, PJoinSmem& sm, int tslot)
                 const u64 off = pc * kHeavyPiece;
                 A.heavy[at + pc] = HeavyItem{p0 + off, ky[k], st[k] + off, (u32)min(kHeavyPiece, cnt[k] - off), (u32)q};
             }
+            atomicAdd((unsigned long long*)&c->heavy_items, (unsigned long long)pieces);
         }
         // light candidates: kPClaim per lane in flight
         for (u32 t0 = 0; t0 < lrun; t0 += 32 * kPClaim) {
