@@ -19,6 +19,10 @@ the driver's peak resident memory.
 Needs the reference tree: --ref, or oracle/Makefile's default (which the
 RA_REFERENCE environment variable overrides); run from the repo root:
     python tests/golden/make_golden.py [--ref <parallel-RA checkout>] [--only NAME ...]
+On a machine without the tree but with oracle/_ref/ref_driver already built
+there (a larger host, for a case whose reference run needs more memory), the
+generated-input cases run with
+    python tests/golden/make_golden.py --prebuilt --only NAME [--out DIR]
 """
 from __future__ import annotations
 
@@ -110,15 +114,26 @@ def main():
     ap.add_argument("--ref", default=O.reference_root(),
                     help="parallel-RA checkout (default: oracle/Makefile's, $RA_REFERENCE)")
     ap.add_argument("--only", nargs="*", help="run only these cases (LARGE cases run only when named)")
+    ap.add_argument("--prebuilt", action="store_true",
+                    help="use the ref_driver already built in oracle/_ref (a machine without the reference "
+                         "tree); generated-input cases only")
+    ap.add_argument("--out", default=HERE, help="directory for the case files (default: beside this script)")
     args = ap.parse_args()
-    if not args.ref or not os.path.isdir(os.path.join(args.ref, "src")):
-        ap.error("give the reference tree with --ref or RA_REFERENCE")
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}", "-j8"], check=True)
-    for name in ("g5955", "g13236"):
-        dst = os.path.join(HERE, f"{name}_edge_2_1_2")
-        shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2"), dst)
-        shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2.size"), dst + ".size")
-    mpath = os.path.join(HERE, "manifest.json")
+    if args.prebuilt:
+        if not os.path.exists(DRIVER):
+            ap.error("--prebuilt: oracle/_ref/ref_driver is not built")
+        if not args.only or any(src[0] == "fixture" for n, _, src in CASES + LARGE_CASES if n in args.only):
+            ap.error("--prebuilt: name generated-input cases with --only")
+    else:
+        if not args.ref or not os.path.isdir(os.path.join(args.ref, "src")):
+            ap.error("give the reference tree with --ref or RA_REFERENCE")
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}", "-j8"],
+                       check=True)
+        for name in ("g5955", "g13236"):
+            dst = os.path.join(HERE, f"{name}_edge_2_1_2")
+            shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2"), dst)
+            shutil.copyfile(os.path.join(args.ref, "data", name, "edge_2_1_2.size"), dst + ".size")
+    mpath = os.path.join(args.out, "manifest.json")
     manifest = json.load(open(mpath)) if os.path.exists(mpath) else {}
     cases = CASES + LARGE_CASES
     if args.only:
@@ -137,7 +152,7 @@ def main():
             case["reference_fixpoint_seconds_1core"] = round(fixpoint, 3)
             case["reference_wall_seconds_1core"] = round(wall, 3)
             case["reference_peak_rss_mb"] = round(resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss / 1024)
-        with open(os.path.join(HERE, f"{name}.json"), "w") as f:
+        with open(os.path.join(args.out, f"{name}.json"), "w") as f:
             json.dump(case, f, separators=(",", ":"))
         manifest[name] = {k: case[k] for k in ("program", "source", "input_rows")}
         print(name, {r: v["count"] for r, v in rels.items()}, "iterations", [len(h[1]) for h in hist],
