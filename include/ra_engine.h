@@ -117,6 +117,8 @@ typedef struct ra_stats {
     uint64_t sliced_passes;     /* join + select passes of those iterations */
     uint64_t heavy_items;       /* work items (2048 candidates each) that join rows with more than 4096
                                    matches were split into, expanded by every block of the launch */
+    uint64_t tail_iterations;   /* iterations run by the tail kernel: small iterations back to back in
+                                   one thread-block cluster, inside the SCC's CUDA graph */
 } ra_stats;
 
 /* Runtime tuning of one program (no counterpart in the reference, whose

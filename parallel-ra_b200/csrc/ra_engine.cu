@@ -19,6 +19,7 @@
 #include "ra_dense.cuh"
 #include "ra_persist.cuh"
 #include "ra_reach.cuh"
+#include "ra_tail.cuh"
 #include "ra_wide.cuh"
 
 #include <algorithm>
@@ -245,6 +246,8 @@ struct ra_program {
     bool use_persist = false;     // RA_PERSIST=1: the persistent SCC kernel instead of CUDA-graph iterations
     bool use_reach = false;       // RA_REACH=1: closure-shaped SCCs by composing reachable sets
     u64 reach_arena_hint = 0;     // arena entries the last reachability evaluation used
+    bool use_tail = true;         // RA_NO_TAIL=1: no tail kernel in the iteration body
+    int tail_ctas = -1;           // CTAs of the tail kernel's cluster (0: none fits; -1: not yet asked)
     bool kernel_events = false;   // RA_KERNEL_EVENTS=1: per-launch events on the claim kernels (no graph)
 };
 
@@ -1165,6 +1168,84 @@ struct PhaseTimer {
     }
 };
 
+// The tail kernel's cluster: 16 CTAs where the GPU can place such a cluster,
+// else 8 (portable), else none.  Asked once per program, outside any capture.
+void tail_setup(ra_program* p)
+{
+    if (p->tail_ctas >= 0) return;
+    p->tail_ctas = 0;
+    if (cudaFuncSetAttribute(tail_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTailSmem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(tail_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    for (int nc : {kTailMaxCtas, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nc);
+        cfg.blockDim = dim3(kTailThreads);
+        cfg.dynamicSmemBytes = kTailSmem;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = nc;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, tail_cluster_kernel, &cfg) == cudaSuccess && clusters > 0) {
+            p->tail_ctas = nc;
+            return;
+        }
+        cudaGetLastError();
+    }
+}
+
+// Does the iteration body of SCC d start with the tail kernel?  Join rules only
+// (at most kTailMaxRules) into hash seen sets, written straight to the log in
+// emission order, no instances.
+bool tail_ok(ra_program* p, const DevScc& d)
+{
+    if (!p->use_tail || p->tail_ctas <= 0 || p->id_order != RA_IDS_EMISSION || p->n_inst || !d.plan.fixpoint ||
+        d.plan.n_rules > kTailMaxRules)
+        return false;
+    for (const DevRule& r : d.rules)
+        if (r.kind != kJoin || d.bit[r.out_slot].seen || r.in.slot < 0) return false;
+    return true;
+}
+
+void launch_tail(ra_program* p, DevScc& d)
+{
+    TailArgs A{};
+    A.ctl = p->ctl;
+    A.plan = d.plan;
+    A.rm = d.rm;
+    A.n_rules = d.plan.n_rules;
+    for (int q = 0; q < A.n_rules; q++) {
+        const DevRule& r = d.rules[q];
+        Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
+        A.rule[q] = TailRule{r.in, r.outer_shift, r.csr, r.inner, r.pj, out.seen, out.seen_cap, out.keys, out.ids};
+    }
+    A.bits = p->bits;
+    A.cand = p->dcand;
+    A.cand_cap = p->dcand_cap;
+    A.loser = p->dloser;
+    A.history = p->dhist;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p->tail_ctas);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = kTailSmem;
+    cfg.stream = p->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = p->tail_ctas;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, tail_cluster_kernel, A));
+}
+
 // launches of one iteration, in order; returns the number of kernels
 int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, int use_cond)
 {
@@ -1174,6 +1255,9 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
     const bool ref = p->id_order == RA_IDS_REFERENCE;
     int launches = 0;
     int slot = 0;
+    // graph bodies of SCCs the tail kernel serves: the WHILE loop stops before an
+    // iteration small enough for it (the tail kernel follows the loop in the graph)
+    const bool tail = use_cond && tail_ok(p, d);
     for (int q = 0; q < pl.n_rules; q++) {
         const DevRule& r = d.rules[q];
         Relation& out = p->rels[d.rel_of_slot[r.out_slot]];
@@ -1230,6 +1314,12 @@ int launch_iteration(ra_program* p, DevScc& d, cudaGraphConditionalHandle cond, 
         a.dst_ids = ref ? p->stage_v[r.out_slot] : out.ids;
         a.passes = ref ? d.passes[r.out_slot] : 0;
         a.stage_cap = p->stage_cap;
+        if (tail) {
+            a.tail_on = 1;
+            a.tail_nslots = pl.n_rules;
+            for (int t = 0; t < pl.n_rules; t++) a.tail_slot[t] = d.rules[t].in.slot;
+            a.tail_rows = (u64)p->tail_ctas * kTailRowsGo;
+        }
         if (p->n_inst) {
             a.inst_base = p->dinst_base;
             a.n_inst = p->n_inst;
@@ -1850,6 +1940,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     LAUNCHED();
 
     int body_kernels = 0;
+    u64 tail_launches = 0;   // graph launches whose graph ends with the tail kernel
     bool any_bitmap = false;
     for (int sl = 0; sl < pl.n_rels; sl++) any_bitmap = any_bitmap || d.bit[sl].seen;
     // the whole fixed point as one cooperative launch: default id order, hash seen sets
@@ -1873,6 +1964,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 cudaGraphExec_t exec = nullptr;
                 CK(cudaGraphCreate(&graph, 0));
                 cudaGraphConditionalHandle cond;
+                tail_setup(p);
                 CK(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
                 cudaGraphNodeParams cp = {};
                 cp.type = cudaGraphNodeTypeConditional;
@@ -1885,6 +1977,13 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 CK(cudaStreamBeginCaptureToGraph(p->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
                 const int body_kernels_captured = launch_iteration(p, d, cond, 1);
                 CK(cudaStreamEndCapture(p->stream, &body));
+                if (tail_ok(p, d)) {
+                    // the tail kernel after the loop: the small iterations that end it
+                    CK(cudaStreamBeginCaptureToGraph(p->stream, graph, &node, nullptr, 1,
+                                                     cudaStreamCaptureModeRelaxed));
+                    launch_tail(p, d);
+                    CK(cudaStreamEndCapture(p->stream, &graph));
+                }
                 CK(cudaGraphInstantiate(&exec, graph, 0));
                 s.graph = graph;
                 s.exec = exec;
@@ -1896,6 +1995,7 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
                 s.graph_kernels = body_kernels_captured;
             }
             body_kernels = s.graph_kernels;
+            if (tail_ok(p, d)) tail_launches++;
             CK(cudaGraphLaunch(s.exec, p->stream));
             ctl_download(p);
         } else {
@@ -2049,8 +2149,10 @@ void run_scc_device(ra_program* p, Scc& s, DevScc& d)
     p->stats.iterations += h.iteration;
     p->stats.join_candidates += h.candidates;
     p->stats.heavy_items += h.heavy_items;
+    p->stats.tail_iterations += h.tail_iters;
     p->stats.new_tuples += h.new_tuples;
-    p->stats.kernel_launches += (u64)body_kernels * h.iteration;
+    // loop bodies for the iterations the loop ran, one tail kernel per graph launch that has it
+    p->stats.kernel_launches += (u64)body_kernels * (h.iteration - h.tail_iters) + tail_launches;
     p->stats.dedup_launches += (u64)d.rules.size() * h.iteration;
     p->stats.dedup_bytes += 48 * h.candidates + 24 * h.outer_rows;
     p->history.push_back((uint64_t)s.id);
@@ -3043,6 +3145,7 @@ int ra_program_create(int device, ra_program** out)
         dev_alloc(p, &p->ctl, 1);
         CK(cudaMallocHost(&p->hctl, sizeof(IterCtl)));
         if (const char* e = getenv("RA_NO_GRAPH")) p->use_graphs = atoi(e) == 0;
+        if (const char* e = getenv("RA_NO_TAIL")) p->use_tail = atoi(e) == 0;
         if (const char* e = getenv("RA_PERSIST")) p->use_persist = atoi(e) != 0;
         if (const char* e = getenv("RA_REACH")) p->use_reach = atoi(e) != 0;
         if (const char* e = getenv("RA_KERNEL_EVENTS")) p->kernel_events = atoi(e) != 0;

@@ -33,6 +33,7 @@ constexpr int kMaxSccRules = 8;
 constexpr int kMaxTagSlots = 8;
 constexpr int kMaxPasses = 8;
 constexpr int kTileSlots = 128;
+constexpr int kTailMaxRules = 2;   // join rules of an SCC the tail kernel (ra_tail.cuh) runs
 // a bank of launch counters: kTileSlots tile counters, then 3 heavy-row counters per rule
 constexpr int kBankWords = kTileSlots + 3 * kMaxSccRules;
 
@@ -67,6 +68,8 @@ struct IterCtl {
     u64 heavy_n;                    // items pushed
     u64 ns_claims, ns_heavy, ns_select;   // device time of the phases of the persistent kernel (ns)
     u64 t_phase;                    // %globaltimer at the last barrier release (or kernel start)
+    u64 tail_iters;                 // iterations run by the tail kernel (ra_tail.cuh)
+    u64 tail_off;                   // the tail kernel declined a skewed iteration: no more tail in this SCC run
     u32 bar_count;                  // blocks arrived at the running barrier
     u32 bar_gen;                    // barrier generation (bumped on release)
     u32 bar_flags;                  // flags / done / heavy_n as the last arriver saw them
@@ -694,7 +697,7 @@ __global__ void __launch_bounds__(kThreads, RA_JOIN_MIN_BLOCKS) join_fused_kerne
                                                               HeavyItem* __restrict__ heavy, u64 heavy_cap)
 {
     __shared__ JoinSmem S;
-    if (ctl->flags) return;
+    if (ctl->flags || ctl->done) return;   // done: the tail kernel reached the fixed point
     const u64 n = sl.on ? sl.rows : rows_n(ctl, outer_ref);
     const u64* outer = rows_ptr(ctl, outer_ref) + (sl.on ? sl.lo : 0);
     if (n == 0) {
@@ -738,7 +741,7 @@ __global__ void __launch_bounds__(kThreads) copy_claim_kernel(IterCtl* __restric
                                                               Slot* __restrict__ seen, u64 seen_cap,
                                                               u32* __restrict__ loser, BitSeen bs)
 {
-    if (ctl->flags) return;
+    if (ctl->flags || ctl->done) return;
     const u64 c = rows_n(ctl, in_ref);
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cand_n[rule] = c;
     if (c == 0) return;
@@ -887,7 +890,22 @@ struct SelectArgs {
     int inst_shift;           // bit offset of column 0 in the output relation's key
     u64* inst_new;            // [iteration][instance] counts of new tuples
     u64 inst_iter_cap;
+    // the tail kernel (ra_tail.cuh) follows the graph's WHILE loop: the iteration end
+    // stops the loop when every join rule's next outer delta has at most tail_rows rows
+    int tail_on;
+    int tail_nslots;
+    int tail_slot[kTailMaxRules];
+    u64 tail_rows;
 };
+
+// Does the next iteration go to the tail kernel?  (After the iteration end: not
+// done, no flag, every join rule's next delta small.)
+__device__ __forceinline__ bool tail_next(const IterCtl* c, const SelectArgs& a)
+{
+    bool small = c->flags == 0 && c->done == 0 && c->tail_off == 0;
+    for (int i = 0; i < a.tail_nslots; i++) small = small && c->delta_n[a.tail_slot[i]] <= a.tail_rows;
+    return small;
+}
 
 // instance owning value v (inst_base sorted, n + 1 entries)
 __device__ __forceinline__ u32 instance_of(const u64* __restrict__ base, u32 n, u64 v)
@@ -931,6 +949,7 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
     __shared__ u32 s_tile;
     __shared__ u64 s_prefix;
     __shared__ u32 s_hist[kMaxPasses][kRadix];
+    if (ctl->done) return;   // the tail kernel reached the fixed point in this body
     const int rule = a.rule;
     const u64 c = ctl->cand_n[rule];
     const int out = plan.rule_out[rule], tslot = plan.rule_tag[rule];
@@ -1053,7 +1072,10 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
         if (done == parting - 1) {
             __threadfence();
             ctl->exit_ctr = 0;
-            if (a.last) end_of_iteration(ctl, plan, rm, history, cond, use_cond);
+            if (a.last) {
+                end_of_iteration(ctl, plan, rm, history, cond, use_cond);
+                if (a.tail_on && use_cond && tail_next(ctl, a)) cudaGraphSetConditional(cond, 0u);
+            }
         }
     }
 }

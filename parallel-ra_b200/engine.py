@@ -57,7 +57,7 @@ class Stats(C.Structure):
         ("dense_emit_ms", C.c_double), ("bitmap_relations", C.c_uint64),
         ("persistent_launches", C.c_uint64), ("reach_sccs", C.c_uint64), ("reach_levels", C.c_uint64),
         ("reach_ms", C.c_double), ("reach_phase_ms", C.c_double * 4), ("sliced_iterations", C.c_uint64),
-        ("sliced_passes", C.c_uint64), ("heavy_items", C.c_uint64),
+        ("sliced_passes", C.c_uint64), ("heavy_items", C.c_uint64), ("tail_iterations", C.c_uint64),
     ]
     PHASES = ("join_scan", "plan", "expand_claim", "select", "sort", "iter_end")
 
