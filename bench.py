@@ -57,10 +57,11 @@ INPUT = {"tc": "G", "sg": "edge"}
 # bounded CPU samples of the same graph families (the cpu_baseline of our arm, and the
 # reference arm of workloads in REFERENCE_SAMPLED)
 CPU_SAMPLES = {"tc": ("er", (1 << 17, round(0.95 * (1 << 17)), 2)), "sg": ("tree", (1 << 12, 3))}
-# the reference's same generation on the 2^15-node tree holds ~4.6e8 tuples in its B-tree
-# tries: about 70 GB of host memory (1.51 GB measured for the 2^12-node tree's 9.8e6), more
-# than the box offers the arm; its reference arm runs the 2^12-node sample instead
-REFERENCE_SAMPLED = {"sg-tree15"}
+# the reference's same generation on the 2^15-node tree holds 5.5e8 tuples in its B-tree
+# tries: a 73.7 GB peak (measured when its golden was generated, 694 s of fixpoint on one
+# core); on a host with less free memory than the figure below, its reference arm
+# runs the 2^12-node sample instead
+REFERENCE_SAMPLED = {"sg-tree15": 96 << 30}
 REFERENCE_ARM_SECONDS = 600.0
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
@@ -228,6 +229,18 @@ def metric_of(kind):
     return f"{OUTPUT[kind]} tuples/s" if kind == "sg" else METRIC
 
 
+def host_free_bytes() -> int:
+    """Host memory available to a new process (MemAvailable), 0 if unknown."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return None
@@ -283,8 +296,8 @@ def run_reference_arm(args, rank, world):
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "instances/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
     prog_kind, gen, params = WORKLOADS[args.workload]
-    if args.workload in REFERENCE_SAMPLED:
-        # the reference needs more host memory than this workload's input allows (see REFERENCE_SAMPLED)
+    if args.workload in REFERENCE_SAMPLED and host_free_bytes() < REFERENCE_SAMPLED[args.workload]:
+        # the reference needs more host memory than this host has free (see REFERENCE_SAMPLED)
         rows, desc, same = None, cpu_sample_desc(prog_kind), False
     else:
         rows = workload_rows(gen, params)
