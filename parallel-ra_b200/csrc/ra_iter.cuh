@@ -945,10 +945,12 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
                                                           u64* __restrict__ history, cudaGraphConditionalHandle cond,
                                                           int use_cond)
 {
+    static_assert(kSelIpt == 4, "select loads a thread's candidates as 2 x 16 bytes and its marks as 16 bytes");
     __shared__ u64 sm[kWarps + 1];
     __shared__ u32 s_tile;
     __shared__ u64 s_prefix;
     __shared__ u32 s_hist[kMaxPasses][kRadix];
+    __shared__ u64 s_win[kSelTile];   // the tile's winners, compacted, for coalesced stores
     if (ctl->done) return;   // the tail kernel reached the fixed point in this body
     const int rule = a.rule;
     const u64 c = ctl->cand_n[rule];
@@ -998,6 +1000,7 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
         const u64 cbase = a.sliced ? 0 : stream_base(ctl, rule);
         const u32 ep = (u32)ctl->epoch;
         const u64* in = cand + cbase;
+        const bool aligned = (cbase & 3) == 0;   // 16-byte vector loads of candidates and marks
         const u32 tag = iter_tag(ctl, tile_slot);
         u32* ctr = tile_counter(ctl, tile_slot);
         for (int i = threadIdx.x; i < a.passes * kRadix; i += kThreads) (&s_hist[0][0])[i] = 0;
@@ -1009,42 +1012,56 @@ __global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(
             if (tile >= ntiles) break;
             const u64 base = tile * kSelTile + (u64)threadIdx.x * kSelIpt;
             u64 key[kSelIpt];
+            u32 mk[kSelIpt];
+            if (aligned && base + kSelIpt <= c) {
+                // a thread's 4 candidates and their marks in three 16-byte loads
+                const ulonglong2 k01 = *(const ulonglong2*)(in + base), k23 = *(const ulonglong2*)(in + base + 2);
+                const uint4 m = *(const uint4*)(loser + cbase + base);
+                key[0] = k01.x; key[1] = k01.y; key[2] = k23.x; key[3] = k23.y;
+                mk[0] = m.x; mk[1] = m.y; mk[2] = m.z; mk[3] = m.w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < kSelIpt; k++) {
+                    const bool v = base + k < c;
+                    key[k] = v ? in[base + k] : kEmpty;
+                    mk[k] = v ? loser[cbase + base + k] : ep;
+                }
+            }
             u32 win = 0;
 #pragma unroll
             for (int k = 0; k < kSelIpt; k++) {
-                const u64 p = base + k;
-                key[k] = kEmpty;
-                if (p < c) {
-                    const u64 kk = in[p];
-                    if (kk != kEmpty && loser[cbase + p] != ep) {
-                        key[k] = kk;
-                        win++;
-                    }
-                }
+                if (key[k] == kEmpty || mk[k] == ep) key[k] = kEmpty;
+                else win++;
             }
             u64 agg;
-            u64 ex = block_exclusive_scan((u64)win, sm, &agg);
+            const u64 ex = block_exclusive_scan((u64)win, sm, &agg);
             if (threadIdx.x < 32) {
                 const u64 pre = lookback_warp(status, (u32)tile, agg, tag, &ctl->flags);
                 if (threadIdx.x == 0) s_prefix = pre;
             }
-            __syncthreads();
-            u64 r = s_prefix + ex;
+            {   // compacted into shared memory meanwhile
+                u64 e = ex;
 #pragma unroll
-            for (int k = 0; k < kSelIpt; k++) {
-                if (key[k] == kEmpty) continue;
-                dk[dst_off + r] = key[k];
+                for (int k = 0; k < kSelIpt; k++)
+                    if (key[k] != kEmpty) s_win[e++] = key[k];
+            }
+            __syncthreads();
+            const u64 pre = s_prefix;
+            // the tile's winners: log rows dst_off + pre + i, consecutive threads, consecutive rows
+            for (u32 i = threadIdx.x; i < agg; i += kThreads) {
+                const u64 kk = s_win[i];
+                const u64 r = pre + i;
+                dk[dst_off + r] = kk;
                 dv[dst_off + r] = tag_word | (id_ctr + r);
                 for (int ps = 0; ps < a.passes; ps++)
-                    atomicAdd(&s_hist[ps][(key[k] >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
-                r++;
+                    atomicAdd(&s_hist[ps][(kk >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
             }
             if (a.inst_base) {
                 u64* row = a.inst_new + ctl->iteration * a.n_inst;
-#pragma unroll
-                for (int k = 0; k < kSelIpt; k++) {
-                    const bool v = key[k] != kEmpty;
-                    const u32 inst = v ? instance_of(a.inst_base, a.n_inst, key[k] >> a.inst_shift)
+                for (u32 i0 = 0; i0 < agg; i0 += kThreads) {   // warp-uniform trip count
+                    const u32 i = i0 + threadIdx.x;
+                    const bool v = i < agg;
+                    const u32 inst = v ? instance_of(a.inst_base, a.n_inst, s_win[i] >> a.inst_shift)
                                        : (0x80000000u | (u32)threadIdx.x);
                     const u32 peers = __match_any_sync(0xffffffffu, inst);
                     if (v && (peers & lanemask_lt()) == 0) atomicAdd(&row[inst], (u64)__popc(peers));
