@@ -149,7 +149,7 @@ struct ra_program {
     bool own_stream = false;
     uint32_t batch_size = 1;
     int id_order = RA_IDS_EMISSION;
-    ra_tuning tune = {0.45, 4.0, 1.5, 4, 4, 8e9};   // the autotuner's B200 choice (tuning.json)
+    ra_tuning tune = {0.45, 4.0, 1.5, 8, 4, 8e9};   // the B200 choice (tuning.json)
     std::vector<Relation> rels;
     std::vector<Scc> sccs;
     std::vector<std::pair<int, int>> deps;
