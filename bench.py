@@ -65,10 +65,10 @@ REFERENCE_SAMPLED = {"sg-tree15": 96 << 30}
 REFERENCE_ARM_SECONDS = 600.0
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per algorithmic byte of join_fused_kernel, from the
-# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.86 / 1.87 / 1.87 over
+# ncu capture in profiles/join_fused_kernel_tc-er20.md (1.93 / 1.93 / 1.95 over
 # three launches of the same graph family at 1/4 scale); bench's `traffic` is
 # this ratio times the algorithmic bytes of an average tc-er22 launch.
-TRAFFIC_PER_ALGO_BYTE = 1.87
+TRAFFIC_PER_ALGO_BYTE = 1.94
 
 
 def load_peaks():
@@ -468,15 +468,19 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = load_peaks()
     achieved = (dedup_bytes / dedup_launches) / ((dedup_ms / dedup_launches) / 1e3) / 1e9 if dedup_launches else 0.0
+    bitmap = st.bitmap_relations > 0
     roofline = dense_roofline(dense, peak, peak_kind) if dense["sccs"] else {"kernel": "join_fused_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": TRAFFIC_PER_ALGO_BYTE * dedup_bytes / max(dedup_launches, 1),
-                "traffic_note": "ncu DRAM read+write per launch, measured on tc-er20 and scaled by units processed",
+                "traffic": None if bitmap else TRAFFIC_PER_ALGO_BYTE * dedup_bytes / max(dedup_launches, 1),
+                "traffic_note": ("not captured for the bitmap path" if bitmap else
+                                 "ncu DRAM read+write per launch, measured on tc-er20 and scaled by units processed"),
                 "launches": int(dedup_launches), "avg_launch_us": 1e3 * dedup_ms / max(dedup_launches, 1),
                 "bytes_per_launch": dedup_bytes / max(dedup_launches, 1),
-                "bytes_model": "48 B per candidate (8 B inner key read, 8 B candidate write, 16 B seen-slot read "
-                               "+ 16 B write) + 24 B per outer delta row (key, row offset, CSR start)"}
-    if not dense["sccs"] and dedup_launches and world == 1:
+                "bytes_model": ("8 B per candidate (the inner key; the claim is a bit test and an atomicOr on a "
+                                "bitmap word, mostly L2-resident) + 24 B per outer delta row" if bitmap else
+                                "48 B per candidate (8 B inner key read, 8 B candidate write, 16 B seen-slot read "
+                                "+ 16 B write) + 24 B per outer delta row (key, row offset, CSR start)")}
+    if not dense["sccs"] and not bitmap and dedup_launches and world == 1:
         # the claims' own ceiling on this GPU: random 16-byte CAS on a table of the seen set's size
         cal = P.engine.calibrate_random_access(dev, slots=max(1 << 20, int(tc / 0.45)), ops=64 << 20)
         claims_per_s = st.join_candidates / (dedup_ms / max(1, min(args.steps, 3)) / 1e3) if dedup_ms else 0.0
