@@ -41,9 +41,10 @@ constexpr int kTailRowsPerCta = kTailThreads * kTailRowsPerThread;   // capacity
 // An iteration goes to the tail kernel when every rule's outer delta has at most
 // kTailRowsGo rows per CTA of the cluster.  Claims are bound by each SM's rate of
 // random 16-byte atomics (the device's ~21 G/s is ~0.15 G/s per SM), so the rows
-// are spread evenly over the CTAs, and larger iterations, which the join launch
-// spreads over every SM, stay on the graph path.
-constexpr int kTailRowsGo = 512;
+// are spread evenly over the CTAs.  Measured on tc-er22 (ms per step, same box):
+// 256 rows per CTA 12.15, 512 12.07, 1,024 11.97, 2,048 11.66; a variant with 4
+// rows per thread and 4,096 rows per CTA 11.79.
+constexpr int kTailRowsGo = kTailRowsPerCta;
 constexpr u64 kTailCtaCands = 32768;   // a CTA's candidates per rule, above which the graph path is faster
 constexpr int kTailMaxCtas = 16;
 // dynamic shared memory: exclusive match prefix (rows + 1), first inner row and key per row

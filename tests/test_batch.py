@@ -117,6 +117,40 @@ def test_tc_wave_matches_plain_and_oracle():
     plain.close()
 
 
+def instance_rows(rows, base, i, arity):
+    """Instance i's rows of a union relation dump: data columns in [base[i], base[i+1]),
+    rebased to 0, in trie order (ids dropped: a wave numbers its ids across instances)."""
+    lo = int(base[i])
+    hi = int(base[i + 1]) if i + 1 < len(base) else 1 << 62
+    d = rows[:, :arity].astype(np.int64)
+    sel = (d[:, 0] >= lo) & (d[:, 0] < hi)
+    out = d[sel] - lo
+    return out[np.lexsort(out.T[::-1])] if out.shape[0] else out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["tc", "sg"])
+def test_wave_rows_equal_plain_runs(kind):
+    """Row for row, every relation of every instance of a wave equals a plain single-instance run's."""
+    if kind == "tc":
+        insts = small_instances(24, 5)
+    else:
+        insts = [P.datagen.with_row_ids(P.datagen.random_tree(n, 300 + n)) for n in (3, 40, 200, 700)]
+    wave = P.batch.Runner(kind)
+    base = wave.load_wave(insts)
+    wave.prog.execute()
+    dumps = {name: wave.prog.dump_full(h) for name, h in wave.rels.items()}
+    plain = P.batch.Runner(kind)
+    for i, rows in enumerate(insts):
+        plain.run_plain(rows)
+        for name, h in plain.rels.items():
+            want = plain.prog.dump_full(h)[:, :2].astype(np.int64)
+            got = instance_rows(dumps[name], base, i, 2)
+            assert np.array_equal(got, want), (i, name)
+    wave.close()
+    plain.close()
+
+
 @pytest.mark.gpu
 def test_sg_wave_matches_plain_and_oracle():
     insts = [P.datagen.with_row_ids(P.datagen.random_tree(n, 100 + n)) for n in (2, 17, 64, 200, 513, 1000)]
