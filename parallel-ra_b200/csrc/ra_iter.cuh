@@ -9,10 +9,11 @@
 //   join_fused     per tile of outer (delta) rows: match counts from the inner
 //                  CSR, single-pass decoupled look-back scan of the counts, then
 //                  the tile's candidates expanded in place (merge-path over the
-//                  tile's rows, so a heavy row is spread over all the block's
-//                  warps), written to the candidate stream and claimed in the
-//                  output relation's seen set (first occurrence = least stream
-//                  position) -- count, scan and write in one launch
+//                  tile's rows, so a row is spread over all the block's warps;
+//                  a row of more than kHeavyRow matches goes to every block of
+//                  the launch as work items), written to the candidate stream and
+//                  claimed in the output relation's seen set (first occurrence =
+//                  least stream position) -- count, scan and write in one launch
 //   copy_claim     (copy / copy_filter rules) one candidate per input row
 //   select         per candidate: winner test, ordered compaction (look-back)
 //                  straight into the relation's log, intern ids; the last tile
