@@ -944,8 +944,11 @@ __global__ void __launch_bounds__(kThreads) bitmap_tables_kernel(const u64* __re
     }
 }
 
-__global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(IterCtl* __restrict__ ctl, SccPlan plan, SccRelMap rm,
-                                                          SelectArgs a, const u64* __restrict__ cand,
+__global__ void __launch_bounds__(kThreads, RA_SELECT_MIN_BLOCKS) select_kernel(IterCtl* __restrict__ ctl,
+                                                          // read in place from the parameter space (indexed by rule / relation)
+                                                          const __grid_constant__ SccPlan plan,
+                                                          const __grid_constant__ SccRelMap rm,
+                                                          const __grid_constant__ SelectArgs a, const u64* __restrict__ cand,
                                                           const u32* __restrict__ loser,
                                                           u64* __restrict__ status, int tile_slot,
                                                           u64* __restrict__ history, cudaGraphConditionalHandle cond,
